@@ -1,0 +1,195 @@
+/*
+ * scphd.h — C ABI of the B200 SC-PHD camera-calibration filter step.
+ *
+ * One handle = one filter: N parent particles (12-D camera extrinsics, FP64) each
+ * owning a Gaussian-mixture map in 6-D disparity space (u, v, d, vu, vv, vd).
+ * The entry points replace the step API of the reference class
+ * SCPHDCameraCalibration (src/scphdcameracalibration.cuh:29-44):
+ *
+ *   reference                                   this ABI
+ *   SCPHDCameraCalibration(cfg)  (.cu:823-1006) scphd_create
+ *   predict(double dt)           (.cu:1034-1151) scphd_predict
+ *   update(u, v, fixed_camera)   (.cu:1576-2094) scphd_update (d == NULL: (u,v) mode)
+ *   resample()                   (.cu:2651-2817) scphd_resample
+ *   checkStuff()                 (.cu:812-821)   scphd_check
+ *   writeMat() particle dump     (.cu:2200-2373) scphd_get_particles / scphd_get_mixture
+ *
+ * Conventions: every call returns an scphd_status and never throws across the ABI.
+ * Host arrays are copied during the call (the reference passes measurements by
+ * value).  All device work of a handle runs on the handle's own CUDA stream; calls
+ * on distinct handles may come from distinct threads, calls on one handle must be
+ * serialised by the caller.  Memory is allocated once, in scphd_create, from the
+ * capacities in scphd_config; no call allocates afterwards.
+ */
+#ifndef SCPHD_H
+#define SCPHD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum scphd_status {
+    SCPHD_OK = 0,
+    SCPHD_ERR_INVALID = 1,      /* bad argument or configuration */
+    SCPHD_ERR_CUDA = 2,         /* CUDA runtime error (message in scphd_last_error) */
+    SCPHD_ERR_CAPACITY = 3,     /* a size exceeds the capacity fixed at create time */
+    SCPHD_ERR_NAN = 4,          /* scphd_check found a NaN parent weight */
+    SCPHD_ERR_NO_DEVICE = 5
+} scphd_status;
+
+/* Arithmetic of the Kalman update, merge and sample clouds.  Parent states,
+ * parent log-weights, the log-likelihood accumulation and the resampling prefix
+ * sum are FP64 in both modes. */
+enum { SCPHD_FP32 = 0, SCPHD_FP64 = 1 };
+
+/* Filter configuration.  Field names follow the keys the reference reads through
+ * libconfig (src/scphdcameracalibration.cu:827-1005, 1145, 1343, 1744, 1920,
+ * 2596-2610, 2655); the capacity fields, meas_dim, std_d, baseline, kappa,
+ * precision and seed are additions of this implementation. */
+typedef struct scphd_config {
+    int32_t n_parents;              /* n_particles */
+    int32_t particles_per_feature;  /* Monte-Carlo samples per daughter Gaussian, <= 256 */
+    int32_t max_gaussians;          /* per-parent map capacity (G_max) */
+    int32_t max_measurements;       /* per-frame measurement capacity (M_max) */
+    int32_t meas_dim;               /* 2: (u,v) as the reference; 3: (u,v,d) */
+    int32_t precision;              /* SCPHD_FP32 or SCPHD_FP64 */
+    int32_t max_survivors;          /* per-parent merge scratch; 0 = 4*max_gaussians+max_measurements */
+    int32_t device;                 /* CUDA device ordinal */
+    uint64_t seed;                  /* key of the counter-based random streams */
+    /* prior.{cartesian,angular}.{x,y,z,vx,vy,vz}.{a,b}: uniform prior box */
+    double prior_a[12];
+    double prior_b[12];
+    /* camera_motion_model.{cartesian,angular}.{ax,ay,az} (acceleration std) */
+    double cam_std[6];
+    /* feature_motion_model.{ax,ay,az} */
+    double feat_std[3];
+    /* measurement_model.{fx,fy,u0,v0,std_u,std_v,pd}; std_d for meas_dim 3 */
+    double fx, fy, u0, v0, std_u, std_v, std_d, pd;
+    double kappa;                   /* clutter density; the reference uses lambda/(2 v0)^2 */
+    double baseline;                /* stereo baseline B in d = -fx B / z; 1 reproduces the reference */
+    double ps;                      /* survival probability */
+    double min_weight;              /* prune threshold */
+    double min_separation;          /* squared Mahalanobis merge threshold */
+    double min_neff;                /* resample when N_eff/N < min_neff */
+    /* birth.{w0,d0,vu0,vv0,vd0,var_d0,var_vu0,var_vv0,var_vd0} */
+    double w0, d0, vu0, vv0, vd0, var_d0, var_vu0, var_vv0, var_vd0;
+} scphd_config;
+
+typedef struct scphd_filter scphd_filter;
+
+/* Fill *cfg with the values of the reference's shipped config/calibration.cfg
+ * (n_particles 100, particles_per_feature 100, min_weight 1e-4, ...), meas_dim 2,
+ * baseline 1 and kappa = lambda/(2 v0)^2 with lambda 10.0001. */
+void scphd_config_defaults(scphd_config* cfg);
+
+/* SCPHDCameraCalibration(cfg): allocate device state, draw the uniform prior. */
+scphd_status scphd_create(const scphd_config* cfg, scphd_filter** out);
+scphd_status scphd_destroy(scphd_filter* f);
+
+/* predict(dt): parent motion runs now; the feature-cloud motion is fused into the
+ * next scphd_update. */
+scphd_status scphd_predict(scphd_filter* f, double dt);
+
+/* update(u, v, fixed_camera).  u, v (and d when meas_dim == 3) are HOST arrays of n
+ * values.  fixed_camera != 0 transforms with the identity extrinsic and leaves the
+ * parent weights unchanged, as the reference does. */
+scphd_status scphd_update(scphd_filter* f, const double* u, const double* v,
+                          const double* d, int32_t n, int32_t fixed_camera);
+
+/* Same as scphd_update with DEVICE arrays (FP64, n values each; d may be NULL). */
+scphd_status scphd_update_device(scphd_filter* f, const double* u_dev, const double* v_dev,
+                                 const double* d_dev, int32_t n, int32_t fixed_camera);
+
+/* resample(): systematic resampling when N_eff/N < min_neff.  *resampled (may be
+ * NULL) receives 1 if it happened; the decision is read back from the device. */
+scphd_status scphd_resample(scphd_filter* f, int32_t* resampled);
+
+/* predict + update + resample in one call with no host synchronisation inside:
+ * the resampling decision stays on the device.  Host measurement arrays. */
+scphd_status scphd_step(scphd_filter* f, double dt, const double* u, const double* v,
+                        const double* d, int32_t n, int32_t fixed_camera);
+
+/* checkStuff(): SCPHD_ERR_NAN if any parent weight is NaN. */
+scphd_status scphd_check(scphd_filter* f);
+
+/* Wait for the handle's stream. */
+scphd_status scphd_synchronize(scphd_filter* f);
+
+/* Parent states (n_parents x 12 FP64: cartesian x,y,z,vx,vy,vz, angular x,y,z,vx,vy,vz)
+ * and normalised log-weights (n_parents FP64).  Either pointer may be NULL. */
+scphd_status scphd_get_particles(scphd_filter* f, double* states, double* log_weights);
+
+/* Map size of each parent (n_parents int32). */
+scphd_status scphd_get_map_sizes(scphd_filter* f, int32_t* sizes);
+
+/* Gaussian weights of parent p's map (sizes[p] FP64). */
+scphd_status scphd_get_map_weights(scphd_filter* f, int32_t p, double* weights);
+
+/* Euclidean sample cloud of parent p's map: sizes[p] x 6 x particles_per_feature
+ * coordinates (x,y,z,vx,vy,vz) and sizes[p] x particles_per_feature sample
+ * weights, FP64.  Merged components are regenerated from their stored parameters
+ * with the same random streams the next update consumes. */
+scphd_status scphd_get_map_clouds(scphd_filter* f, int32_t p, double* xyz, double* omega);
+
+/* Inspection of the last update (the reference's save_all_maps dumps):
+ * which = SCPHD_MIX_FITTED: the predicted mixture refitted in disparity space,
+ *         per Gaussian 29 values: weight, mean pD, mean[6], packed lower cov[21];
+ * which = SCPHD_MIX_MERGED: the merged mixture, per Gaussian 28 values: weight,
+ *         mean[6], packed lower cov[21].  *count receives the number of rows;
+ * out may be NULL to query the count. */
+enum { SCPHD_MIX_FITTED = 0, SCPHD_MIX_MERGED = 1 };
+scphd_status scphd_get_mixture(scphd_filter* f, int32_t which, int32_t p,
+                               double* out, int32_t* count);
+
+/* Per-(parent, measurement) log normalisers of the last update (n_parents x n FP64)
+ * and per-parent log-likelihood increments (n_parents FP64). */
+scphd_status scphd_get_normalizers(scphd_filter* f, double* ell, double* loglik);
+
+/* Resampling indices of the last resample that happened (n_parents int32). */
+scphd_status scphd_get_resample_indices(scphd_filter* f, int32_t* idx);
+
+/* Replace the filter state: parent states (N x 12), log-weights (N), and per parent
+ * a map given as Euclidean clouds: sizes (N), weights (sum sizes), clouds
+ * (sum sizes x 6 x P_f) and sample weights (sum sizes x P_f).  Clears any
+ * pending prediction.  Used to start device and reference from one state. */
+scphd_status scphd_set_state(scphd_filter* f, const double* states, const double* log_weights,
+                             const int32_t* sizes, const double* weights,
+                             const double* clouds, const double* omega);
+
+/* Counters since create: [0] map truncations at max_gaussians, [1] merge-scratch
+ * overflows at max_survivors, [2] frames updated, [3] resamplings,
+ * [4] Gaussian-measurement units of the last update (sum_p G_p * n),
+ * [5] survivors of the last update (sum over parents). */
+scphd_status scphd_get_counters(scphd_filter* f, int64_t counters[8]);
+
+/* Stand-alone stages on caller-provided HOST data, for parity checks of the
+ * device code paths the step uses.
+ *
+ * scphd_merge_components: the greedy GM reduction of phdUpdateMergeKernel
+ * (src/kernels.cu:662-874) on one list of n components (28 FP64 each: weight,
+ * mean[6], packed lower cov[21]) with prune flags (1 = excluded).  Outputs the
+ * merged list (up to n rows of 28) in *n_out and, per input, the output row it was
+ * absorbed into (-1 if none).  precision selects the FP32 or FP64 device code. */
+scphd_status scphd_merge_components(const double* comps, const uint8_t* flags, int32_t n,
+                                    double min_separation, int32_t precision,
+                                    double* merged, int32_t* n_out, int32_t* member_of);
+
+/* scphd_systematic_resample: the systematic resampling of resample()
+ * (src/scphdcameracalibration.cu:2660-2702) on n linear weights with the offset
+ * u01 * (1/n); writes n indices. */
+scphd_status scphd_systematic_resample(const double* weights, int32_t n, double u01,
+                                       int32_t* idx);
+
+/* Text of the last error on this thread. */
+const char* scphd_last_error(void);
+
+/* Number of CUDA kernels this library launched since load (all handles). */
+int64_t scphd_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SCPHD_H */

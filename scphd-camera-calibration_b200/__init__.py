@@ -1,0 +1,10 @@
+"""B200-native SC-PHD camera-calibration filter step.
+
+The directory name is not a Python identifier; load it with `load_package()` from
+the repository root helpers (bench.py, __graft_entry__.py, tests/conftest.py),
+which registers it as the module `scphd_b200`.
+"""
+from .scphd import (SCPHD_FP32, SCPHD_FP64, SCPHD_MIX_FITTED, SCPHD_MIX_MERGED,  # noqa: F401
+                    SCPHDCameraCalibration, ScphdConfig, ScphdError, kernel_launches,
+                    load_library, merge_components, reference_defaults, systematic_resample)
+from . import scene  # noqa: F401

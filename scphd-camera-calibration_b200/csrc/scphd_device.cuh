@@ -1,0 +1,335 @@
+// scphd_device.cuh — device math of the SC-PHD filter step, templated on the
+// arithmetic type T (float for the fast path, double for the FP64 path).
+//
+// Storage conventions (shared by every kernel):
+//   * a symmetric 6x6 matrix is packed lower-triangular row-major: element (a,b),
+//     a >= b, at a*(a+1)/2 + b (21 values);
+//   * a mixture component row is 32 T: [0] weight, [1..6] mean, [7..27] packed cov;
+//   * a fitted row is 32 T: [0] weight, [1] mean pD, [2..7] mean, [8..28] packed cov;
+//   * a prep row (per fitted Gaussian, measurement-independent Kalman terms) is
+//     48 T: [0] log-constant c, [1] PD flag of the posterior cov, [2..7] packed
+//     S^-1 (k x k, packed lower), [8..25] gain K (6 x 3, row-major), [26..46]
+//     packed posterior covariance.
+#pragma once
+
+#include <cstdint>
+#include <cfloat>
+#include <cuda_runtime.h>
+
+namespace scphd {
+
+constexpr int kRow = 32;
+constexpr int kPrep = 48;
+constexpr int kPrepSi = 2, kPrepK = 8, kPrepCov = 26;
+constexpr int kMaxLanesSamples = 8;   // particles_per_feature <= 256
+
+enum Stage : uint32_t { ST_PRIOR = 1, ST_CAM = 2, ST_FEAT = 3, ST_SAMPLE = 4, ST_RESAMPLE = 5 };
+
+__host__ __device__ inline int tri(int a, int b) { return a >= b ? a * (a + 1) / 2 + b : b * (b + 1) / 2 + a; }
+
+__host__ __device__ inline uint32_t ctr_word3(uint32_t frame, uint32_t stage, uint32_t block) {
+    return (frame << 12) | (stage << 8) | block;
+}
+
+// Philox4x32-10 (Salmon et al., SC'11), counter (s, j, p, c3), key = seed
+__host__ __device__ inline void philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                       uint32_t k0, uint32_t k1, uint32_t out[4]) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+#ifdef __CUDA_ARCH__
+        uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+#else
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+#endif
+        uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+__host__ __device__ inline double u01(uint32_t w) { return ((double)w + 0.5) * 0x1p-32; }
+
+// four standard normals (two Box-Muller pairs) from one Philox block
+template <typename T> struct Normals;
+template <> struct Normals<double> {
+    __device__ static void four(const uint32_t w[4], double z[4]) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            double r = sqrt(-2.0 * log(u01(w[2 * h])));
+            double s, c;
+            sincos((2.0 * 3.14159265358979323846) * u01(w[2 * h + 1]), &s, &c);
+            z[2 * h] = r * c;
+            z[2 * h + 1] = r * s;
+        }
+    }
+};
+template <> struct Normals<float> {
+    __device__ static void four(const uint32_t w[4], float z[4]) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            float ua = __fmaf_rn((float)w[2 * h], 0x1p-32f, 0x1p-33f);
+            float ub = __fmaf_rn((float)w[2 * h + 1], 0x1p-32f, 0x1p-33f);
+            ua = fminf(ua, 0.99999994f);
+            float r = sqrtf(-2.0f * logf(ua));
+            float s, c;
+            sincospif(2.0f * ub, &s, &c);
+            z[2 * h] = r * c;
+            z[2 * h + 1] = r * s;
+        }
+    }
+};
+
+template <typename T> __device__ __forceinline__ T tsqrt(T x);
+template <> __device__ __forceinline__ float tsqrt(float x) { return sqrtf(x); }
+template <> __device__ __forceinline__ double tsqrt(double x) { return sqrt(x); }
+template <typename T> __device__ __forceinline__ T texp(T x);
+template <> __device__ __forceinline__ float texp(float x) { return expf(x); }
+template <> __device__ __forceinline__ double texp(double x) { return exp(x); }
+template <typename T> __device__ __forceinline__ T tlog(T x);
+template <> __device__ __forceinline__ float tlog(float x) { return logf(x); }
+template <> __device__ __forceinline__ double tlog(double x) { return log(x); }
+
+template <typename T> __device__ __forceinline__ T tneg_inf();
+template <> __device__ __forceinline__ float tneg_inf() { return -INFINITY; }
+template <> __device__ __forceinline__ double tneg_inf() { return -INFINITY; }
+
+template <typename T> __device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// ------------------------------------------------------------------ camera model
+// Rotation terms of the reference's world<->camera transform
+// (src/disparitymeasurementmodel.cu:3-144), evaluated once per parent in FP64.
+template <typename T> struct Pose {
+    T R[9];    // world->camera rows
+    T t[3];    // camera position in the world
+};
+
+__device__ inline void pose_terms(const double* e12, double R[9]) {
+    double ct, st, cf, sf, cp, sp;
+    sincos(e12[6], &st, &ct);
+    sincos(e12[7], &sf, &cf);
+    sincos(e12[8], &sp, &cp);
+    R[0] = cf * cp; R[1] = ct * sp + st * sf * cp; R[2] = st * sp - ct * sf * cp;
+    R[3] = -cf * sp; R[4] = ct * cp - st * sf * sp; R[5] = st * cp + ct * sf * sp;
+    R[6] = sf; R[7] = -st * cf; R[8] = ct * cf;
+}
+
+template <typename T> __device__ inline Pose<T> make_pose(const double* e12) {
+    double R[9];
+    pose_terms(e12, R);
+    Pose<T> P;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) P.R[i] = (T)R[i];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) P.t[i] = (T)e12[i];
+    return P;
+}
+
+struct Model {   // measurement model constants (FP64 copy; kernels cast to T)
+    double fx, fy, u0, v0, B, pd;
+    double var[3];   // std_u^2, std_v^2, std_d^2
+};
+
+// world point -> (u, v, d, vu, vv, vd), computeMeasurement (:165-196) with baseline B
+template <typename T>
+__device__ inline void measure(const T X[6], const Pose<T>& P, const Model& m, T y[6]) {
+    T d0 = X[0] - P.t[0], d1 = X[1] - P.t[1], d2 = X[2] - P.t[2];
+    T x = P.R[0] * d0 + P.R[1] * d1 + P.R[2] * d2;
+    T yy = P.R[3] * d0 + P.R[4] * d1 + P.R[5] * d2;
+    T z = P.R[6] * d0 + P.R[7] * d1 + P.R[8] * d2;
+    T vx = P.R[0] * X[3] + P.R[1] * X[4] + P.R[2] * X[5];
+    T vy = P.R[3] * X[3] + P.R[4] * X[4] + P.R[5] * X[5];
+    T vz = P.R[6] * X[3] + P.R[7] * X[4] + P.R[8] * X[5];
+    const T fx = (T)m.fx, fy = (T)m.fy, B = (T)m.B;
+    T iz = T(1) / z, iz2 = iz * iz;
+    y[0] = (T)m.u0 - fx * iz * x;
+    y[1] = (T)m.v0 - fy * iz * yy;
+    y[2] = -fx * B * iz;
+    y[3] = -fx * (vx * z - vz * x) * iz2;
+    y[4] = -fy * (vy * z - vz * yy) * iz2;
+    y[5] = fx * B * vz * iz2;
+}
+
+// (u, v, d, vu, vv, vd) -> world point, invertMeasurement (:198-217) with baseline B
+template <typename T>
+__device__ inline void invert(const T y[6], const Pose<T>& P, const Model& m, T X[6]) {
+    const T fx = (T)m.fx, fy = (T)m.fy, B = (T)m.B, u0 = (T)m.u0, v0 = (T)m.v0;
+    T u = y[0], v = y[1], d = y[2], vu = y[3], vv = y[4], vd = y[5];
+    T id = T(1) / d, id2 = id * id, r = fx / fy;
+    T c0 = (u - u0) * B * id;
+    T c1 = r * (v - v0) * B * id;
+    T c2 = -fx * B * id;
+    T c3 = B * (vu * d - vd * (u - u0)) * id2;
+    T c4 = r * (vv * d - vd * (v - v0)) * B * id2;
+    T c5 = fx * B * vd * id2;
+    // camera -> world: X = R^T c + t
+    X[0] = P.R[0] * c0 + P.R[3] * c1 + P.R[6] * c2 + P.t[0];
+    X[1] = P.R[1] * c0 + P.R[4] * c1 + P.R[7] * c2 + P.t[1];
+    X[2] = P.R[2] * c0 + P.R[5] * c1 + P.R[8] * c2 + P.t[2];
+    X[3] = P.R[0] * c3 + P.R[3] * c4 + P.R[6] * c5;
+    X[4] = P.R[1] * c3 + P.R[4] * c4 + P.R[7] * c5;
+    X[5] = P.R[2] * c3 + P.R[5] * c4 + P.R[8] * c5;
+}
+
+template <typename T>
+__device__ inline bool in_range(const T y[6], const Model& m) {   // kernels.cu:37-41
+    return y[0] >= T(0) && y[0] <= T(2 * m.u0) && y[1] >= T(0) && y[1] <= T(2 * m.v0) && y[2] >= T(0);
+}
+
+// ------------------------------------------------------------------ 6x6 algebra
+// Cholesky in the order of src/device_math.cu:123-150 on a packed matrix; returns
+// false if any factor entry is NaN (isPosDef, :800-812).
+template <typename T>
+__device__ inline bool chol6(const T* A, T* L) {
+    bool ok = true;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+#pragma unroll
+        for (int j = 0; j <= i; ++j) {
+            T tmp = A[tri(i, j)];
+            if (i == j) {
+#pragma unroll
+                for (int k = 0; k < j; ++k) tmp -= L[tri(j, k)] * L[tri(j, k)];
+                L[tri(i, i)] = tsqrt(tmp);
+            } else {
+#pragma unroll
+                for (int k = 0; k < j; ++k) tmp -= L[tri(i, k)] * L[tri(j, k)];
+                L[tri(i, j)] = tmp / L[tri(j, j)];
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 21; ++i) ok = ok && !isnan(L[i]);
+    return ok;
+}
+
+// squared Mahalanobis distance of computeMahalDist<6,36> (src/device_math.cu:374-454):
+// Cholesky of (Sa + Sb), triangular inverse (:153-175), sum_i (sum_{j<=i} dj Linv_ij)^2
+template <typename T>
+__device__ inline T mahal6(const T* ma, const T* Sa, const T* mb, const T* Sb) {
+    T S[21], L[21], Li[21], dlt[6];
+#pragma unroll
+    for (int i = 0; i < 21; ++i) S[i] = Sa[i] + Sb[i];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) dlt[i] = ma[i] - mb[i];
+    chol6(S, L);
+#pragma unroll
+    for (int col = 0; col < 6; ++col) {
+#pragma unroll
+        for (int i = col; i < 6; ++i) {
+            T val = (i == col) ? T(1) : T(0);
+#pragma unroll
+            for (int j = col; j < i; ++j) val -= L[tri(i, j)] * Li[tri(j, col)];
+            Li[tri(i, col)] = val / L[tri(i, i)];
+        }
+    }
+    T dist = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        T s = 0;
+#pragma unroll
+        for (int j = 0; j <= i; ++j) s += dlt[j] * Li[tri(i, j)];
+        dist += s * s;
+    }
+    return dist;
+}
+
+// Measurement-independent Kalman terms of one fitted Gaussian for H = [I_K 0],
+// R = diag(var): S^-1, log-constant c = log pD + log w - K/2 log 2pi - 1/2 log det S,
+// gain K = P H' S^-1 and the Joseph-form posterior covariance
+// (I - K H) P (I - K H)' + K R K' of computeDetectionsKernel
+// (src/kernels.cu:506-595), which does not depend on the measurement.
+template <typename T, int K>
+__device__ inline void kalman_prep(const T* fitrow, const Model& m, T* prep) {
+    const T w = fitrow[0], pdbar = fitrow[1];
+    const T* P = fitrow + 8;
+    T S[6], Si[6];
+    S[0] = P[0] + (T)m.var[0];
+    S[1] = P[1];
+    S[2] = P[2] + (T)m.var[1];
+    T det;
+    if (K == 2) {
+        det = S[0] * S[2] - S[1] * S[1];
+        Si[0] = S[2] / det; Si[1] = -S[1] / det; Si[2] = S[0] / det;
+        Si[3] = Si[4] = Si[5] = 0;
+    } else {
+        S[3] = P[3]; S[4] = P[4]; S[5] = P[5] + (T)m.var[2];
+        // packed: S00=S[0], S10=S[1], S11=S[2], S20=S[3], S21=S[4], S22=S[5]
+        T a = S[0], b = S[1], c = S[2], d = S[3], e = S[4], f = S[5];
+        T A00 = c * f - e * e, A10 = d * e - b * f, A11 = a * f - d * d;
+        T A20 = b * e - c * d, A21 = b * d - a * e, A22 = a * c - b * b;
+        det = a * A00 + b * A10 + d * A20;
+        Si[0] = A00 / det; Si[1] = A10 / det; Si[2] = A11 / det;
+        Si[3] = A20 / det; Si[4] = A21 / det; Si[5] = A22 / det;
+    }
+    const T log2pi = (T)1.8378770664093454835606594728112;
+    T c;
+    if (pdbar > T(0) && w > T(0) && det > T(0))
+        c = tlog(pdbar) + tlog(w) - T(0.5) * T(K) * log2pi - T(0.5) * tlog(det);
+    else
+        c = tneg_inf<T>();
+    // gain K[r][cc] = sum_a P[r][a] Si[a][cc]
+    T Kg[18];
+#pragma unroll
+    for (int r = 0; r < 6; ++r)
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+            T s = 0;
+            if (cc < K) {
+#pragma unroll
+                for (int a = 0; a < K; ++a) s += P[tri(r, a)] * Si[tri(a, cc)];
+            }
+            Kg[r * 3 + cc] = s;
+        }
+    // Joseph: P' = P - K(HP) - (HP)'K' + K (HPH') K' + K R K'
+    T Pn[21];
+#pragma unroll
+    for (int a = 0; a < 6; ++a)
+#pragma unroll
+        for (int b = 0; b <= a; ++b) {
+            T s = P[tri(a, b)];
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                s -= Kg[a * 3 + k] * P[tri(k, b)];
+                s -= P[tri(a, k)] * Kg[b * 3 + k];
+                s += Kg[a * 3 + k] * (T)m.var[k] * Kg[b * 3 + k];
+#pragma unroll
+                for (int l = 0; l < K; ++l) s += Kg[a * 3 + k] * P[tri(k, l)] * Kg[b * 3 + l];
+            }
+            Pn[tri(a, b)] = s;
+        }
+    T L[21];
+    bool pdok = chol6(Pn, L);
+    prep[0] = c;
+    prep[1] = pdok ? T(1) : T(0);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) prep[kPrepSi + i] = Si[i];
+#pragma unroll
+    for (int i = 0; i < 18; ++i) prep[kPrepK + i] = Kg[i];
+#pragma unroll
+    for (int i = 0; i < 21; ++i) prep[kPrepCov + i] = Pn[i];
+}
+
+// log-likelihood exponent term c - 1/2 nu' S^-1 nu for measurement z
+template <typename T, int K>
+__device__ __forceinline__ T log_term(T c, const T* Si, const T* mu, const T* z) {
+    T n0 = z[0] - mu[0], n1 = z[1] - mu[1];
+    T q;
+    if (K == 2) {
+        q = Si[0] * n0 * n0 + T(2) * Si[1] * n0 * n1 + Si[2] * n1 * n1;
+    } else {
+        T n2 = z[2] - mu[2];
+        q = Si[0] * n0 * n0 + Si[2] * n1 * n1 + Si[5] * n2 * n2 +
+            T(2) * (Si[1] * n0 * n1 + Si[3] * n0 * n2 + Si[4] * n1 * n2);
+    }
+    return c - T(0.5) * q;
+}
+
+}  // namespace scphd

@@ -1,0 +1,779 @@
+// scphd_filter.cu — host orchestration and C ABI (include/scphd.h) of the B200
+// SC-PHD calibration filter.  One handle owns one CUDA stream and one device
+// arena sized from the configuration at scphd_create; the step API issues
+// kernels only (no allocation, no host synchronisation except where a call
+// returns device data to the host).
+#include "scphd.h"
+#include "scphd_kernels.cuh"
+
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace scphd;
+
+namespace {
+
+thread_local std::string g_err;
+std::atomic<long long> g_launches{0};
+
+scphd_status fail(scphd_status s, const std::string& msg) {
+    g_err = msg;
+    return s;
+}
+
+#define CUDA_TRY(expr)                                                                        \
+    do {                                                                                      \
+        cudaError_t e_ = (expr);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(SCPHD_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define LAUNCHED()                                                                              \
+    do {                                                                                        \
+        g_launches.fetch_add(1, std::memory_order_relaxed);                                     \
+        cudaError_t e_ = cudaGetLastError();                                                    \
+        if (e_ != cudaSuccess) return fail(SCPHD_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+struct Arena {
+    char* base = nullptr;
+    size_t used = 0, cap = 0;
+    template <typename X> X* take(size_t n) {
+        size_t off = (used + 255) & ~(size_t)255;
+        used = off + n * sizeof(X);
+        return base ? reinterpret_cast<X*>(base + off) : nullptr;
+    }
+};
+
+}  // namespace
+
+struct scphd_filter {
+    scphd_config cfg;
+    Params prm;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t stage_ev = nullptr;
+    double* h_stage = nullptr;   // pinned staging of one frame's measurements (3 x Mcap)
+    double* d_stage = nullptr;
+    int cur = 0;
+    uint32_t frame = 0;
+    bool pending = false;
+    double pending_dt = 0;
+    uint32_t pending_frame = 0;
+    uint32_t sample_frame[2] = {0, 0};
+    int last_M = 0;
+    virtual ~scphd_filter() {}
+    virtual scphd_status init() = 0;
+    virtual scphd_status predict(double dt) = 0;
+    virtual scphd_status update_staged(int M, int fixed) = 0;
+    virtual scphd_status resample(int32_t* resampled, bool read_back) = 0;
+    virtual scphd_status get_particles(double* st, double* lw) = 0;
+    virtual scphd_status get_map_sizes(int32_t* sizes) = 0;
+    virtual scphd_status get_map_weights(int p, double* w) = 0;
+    virtual scphd_status get_map_clouds(int p, double* xyz, double* om) = 0;
+    virtual scphd_status get_mixture(int which, int p, double* out, int32_t* count) = 0;
+    virtual scphd_status get_normalizers(double* ell, double* ll) = 0;
+    virtual scphd_status get_resample_indices(int32_t* idx) = 0;
+    virtual scphd_status set_state(const double* st, const double* lw, const int32_t* sizes, const double* w,
+                                   const double* xyz, const double* om) = 0;
+    virtual scphd_status get_counters(int64_t* c) = 0;
+    virtual scphd_status check() = 0;
+};
+
+namespace {
+
+template <typename T> __global__ void k_convert_meas(const double* stage, int M, int has_d, T* z) {
+    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    z[m * 3 + 0] = (T)stage[m];
+    z[m * 3 + 1] = (T)stage[M + m];
+    z[m * 3 + 2] = has_d ? (T)stage[2 * M + m] : T(0);
+}
+
+__global__ void k_iota(int* a, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = i;
+}
+
+__global__ void record_fit_n(const int* map_n, const int* src, int* fit_n, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) fit_n[i] = map_n[src[i]];
+}
+
+__global__ void k_bump(unsigned long long* c, int i) { c[i] += 1; }
+
+__global__ void k_reset_src(int* src, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) src[i] = i;
+}
+
+template <typename T> class Filter final : public scphd_filter {
+public:
+    Bufs<T> b{};
+    void* arena_ptr = nullptr;
+    T* dump = nullptr;        // Gcap x 7 x Ps cloud dump scratch
+    int* fit_n = nullptr;     // N: Gaussians fitted at the last update
+    size_t merge_smem = 0;
+
+    ~Filter() override {
+        if (stream) cudaStreamSynchronize(stream);
+        if (arena_ptr) cudaFree(arena_ptr);
+        if (h_stage) cudaFreeHost(h_stage);
+        if (stage_ev) cudaEventDestroy(stage_ev);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    void carve(Arena& a) {
+        const size_t N = prm.N, G = prm.Gcap, S = prm.Scap, Mc = prm.Mcap, Ps = prm.Ps;
+        b.ext = a.take<double>(N * 12);
+        b.ext_tmp = a.take<double>(N * 12);
+        b.lw = a.take<double>(N);
+        b.src = a.take<int>(N);
+        b.src_tmp = a.take<int>(N);
+        for (int k = 0; k < 2; ++k) {
+            b.map[k] = a.take<T>(N * G * kRow);
+            b.map_ref[k] = a.take<int>(N * G);
+            b.map_n[k] = a.take<int>(N);
+            b.map_ext[k] = a.take<double>(N * 12);
+            b.cloud[k] = a.take<T>(N * G * 7 * Ps);
+        }
+        b.fit = a.take<T>(N * G * kRow);
+        b.prep = a.take<T>(N * G * kPrep);
+        b.z = a.take<T>(Mc * 3);
+        b.ell = a.take<T>(N * Mc);
+        b.surv_r = a.take<int>(N * S);
+        b.surv_w = a.take<T>(N * S);
+        b.surv_n = a.take<int>(N);
+        b.merged = a.take<T>(N * S * kRow);
+        b.merged_n = a.take<int>(N);
+        b.loglik = a.take<double>(N);
+        b.cum = a.take<double>(N);
+        b.scal = a.take<double>(4);
+        b.flags = a.take<int>(4);
+        b.resample_idx = a.take<int>(N);
+        b.counters = a.take<unsigned long long>(8);
+        dump = a.take<T>(G * 7 * Ps);
+        fit_n = a.take<int>(N);
+        d_stage = a.take<double>(Mc * 3);
+    }
+
+    scphd_status init() override {
+        CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&stage_ev, cudaEventDisableTiming));
+        CUDA_TRY(cudaMallocHost(&h_stage, sizeof(double) * 3 * prm.Mcap));
+        Arena probe;
+        carve(probe);
+        void* p = nullptr;
+        cudaError_t e = cudaMalloc(&p, probe.used);
+        if (e != cudaSuccess)
+            return fail(SCPHD_ERR_CAPACITY, "device arena of " + std::to_string(probe.used) +
+                                                " bytes: " + cudaGetErrorString(e));
+        arena_ptr = p;
+        Arena a;
+        a.base = static_cast<char*>(p);
+        a.cap = probe.used;
+        carve(a);
+        CUDA_TRY(cudaMemsetAsync(p, 0, probe.used, stream));
+        merge_smem = (size_t)2 * prm.Scap * (sizeof(T) + 8) + (size_t)6 * prm.Scap * sizeof(T) + prm.Scap + 64;
+        if (prm.K == 2) {
+            CUDA_TRY(cudaFuncSetAttribute(k_merge<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem));
+        } else {
+            CUDA_TRY(cudaFuncSetAttribute(k_merge<T, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem));
+        }
+        const int N = prm.N;
+        k_prior<<<(N + 255) / 256, 256, 0, stream>>>(prm, b.ext, b.lw);
+        LAUNCHED();
+        k_iota<<<(N + 255) / 256, 256, 0, stream>>>(b.src, N);
+        LAUNCHED();
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        return SCPHD_OK;
+    }
+
+    scphd_status materialize_pending() {
+        const int N = prm.N;
+        k_materialize<T><<<N, 256, 0, stream>>>(prm, b, cur, b.cloud[cur ^ 1], b.map[cur ^ 1], b.map_ref[cur ^ 1],
+                                                 b.map_n[cur ^ 1], 1, pending_dt, pending_frame, sample_frame[cur], -1);
+        LAUNCHED();
+        cur ^= 1;
+        k_reset_src<<<(N + 255) / 256, 256, 0, stream>>>(b.src, N);
+        LAUNCHED();
+        pending = false;
+        return SCPHD_OK;
+    }
+
+    scphd_status predict(double dt) override {
+        if (pending) {
+            scphd_status s = materialize_pending();
+            if (s != SCPHD_OK) return s;
+        }
+        frame++;
+        if (frame >= (1u << 20)) return fail(SCPHD_ERR_CAPACITY, "frame counter exhausted (2^20 frames)");
+        const int N = prm.N;
+        k_predict_parents<<<(N + 255) / 256, 256, 0, stream>>>(prm, b.ext, dt, frame);
+        LAUNCHED();
+        pending = true;
+        pending_dt = dt;
+        pending_frame = frame;
+        return SCPHD_OK;
+    }
+
+    template <int K> scphd_status update_k(int M, int fixed) {
+        const int N = prm.N;
+        CUDA_TRY(cudaMemsetAsync(b.counters + 4, 0, 2 * sizeof(unsigned long long), stream));
+        if (prm.P <= 128)
+            k_cloud_fit<T, K, 4><<<N, 256, 0, stream>>>(prm, b, cur, M, fixed, pending ? 1 : 0, pending_dt,
+                                                         pending_frame, sample_frame[cur]);
+        else
+            k_cloud_fit<T, K, 8><<<N, 256, 0, stream>>>(prm, b, cur, M, fixed, pending ? 1 : 0, pending_dt,
+                                                         pending_frame, sample_frame[cur]);
+        LAUNCHED();
+        pending = false;
+        if (M > 0) {
+            dim3 grid(N, (M + 127) / 128);
+            k_likelihood<T, K><<<grid, 128, 0, stream>>>(prm, b, cur, M);
+            LAUNCHED();
+        }
+        k_merge<T, K><<<N, 128, merge_smem, stream>>>(prm, b, cur, M, fixed);
+        LAUNCHED();
+        k_weights<<<1, 1024, 0, stream>>>(N, b.lw, b.loglik, fixed ? 0 : 1, b.scal);
+        LAUNCHED();
+        return SCPHD_OK;
+    }
+
+    scphd_status update_staged(int M, int fixed) override {
+        if (M > 0) {
+            k_convert_meas<T><<<(M + 127) / 128, 128, 0, stream>>>(d_stage, M, prm.K == 3 ? 1 : 0, b.z);
+            LAUNCHED();
+        }
+        // fit_n[p] = G_p for the inspection dumps (taken from the prior map)
+        scphd_status s = prm.K == 2 ? update_k<2>(M, fixed) : update_k<3>(M, fixed);
+        if (s != SCPHD_OK) return s;
+        const int N = prm.N;
+        // fitted counts: the map sizes the update consumed
+        record_fit_n<<<(N + 255) / 256, 256, 0, stream>>>(b.map_n[cur], b.src, fit_n, N);
+        LAUNCHED();
+        cur ^= 1;
+        sample_frame[cur] = frame;
+        k_reset_src<<<(N + 255) / 256, 256, 0, stream>>>(b.src, N);
+        LAUNCHED();
+        last_M = M;
+        bump_counter(2);
+        return SCPHD_OK;
+    }
+
+    void bump_counter(int i) {
+        k_bump<<<1, 1, 0, stream>>>(b.counters, i);
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+    }
+
+    scphd_status resample(int32_t* resampled, bool read_back) override {
+        k_resample<<<1, 1024, 0, stream>>>(prm, b.lw, b.ext, b.ext_tmp, b.src, b.src_tmp, b.cum, b.scal, b.flags,
+                                           b.resample_idx, frame, 0, -1.0, b.counters);
+        LAUNCHED();
+        if (read_back) {
+            int f = 0;
+            CUDA_TRY(cudaMemcpyAsync(&f, b.flags, sizeof(int), cudaMemcpyDeviceToHost, stream));
+            CUDA_TRY(cudaStreamSynchronize(stream));
+            if (resampled) *resampled = f;
+        }
+        return SCPHD_OK;
+    }
+
+    scphd_status get_particles(double* st, double* lw) override {
+        if (st) CUDA_TRY(cudaMemcpyAsync(st, b.ext, sizeof(double) * 12 * prm.N, cudaMemcpyDeviceToHost, stream));
+        if (lw) CUDA_TRY(cudaMemcpyAsync(lw, b.lw, sizeof(double) * prm.N, cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        return SCPHD_OK;
+    }
+
+    scphd_status host_rows(std::vector<int>& src, std::vector<int>& n) {
+        src.resize(prm.N);
+        n.resize(prm.N);
+        CUDA_TRY(cudaMemcpyAsync(src.data(), b.src, sizeof(int) * prm.N, cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaMemcpyAsync(n.data(), b.map_n[cur], sizeof(int) * prm.N, cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        return SCPHD_OK;
+    }
+
+    scphd_status get_map_sizes(int32_t* sizes) override {
+        std::vector<int> src, n;
+        scphd_status s = host_rows(src, n);
+        if (s != SCPHD_OK) return s;
+        for (int p = 0; p < prm.N; ++p) sizes[p] = n[src[p]];
+        return SCPHD_OK;
+    }
+
+    scphd_status get_map_weights(int p, double* w) override {
+        std::vector<int> src, n;
+        scphd_status s = host_rows(src, n);
+        if (s != SCPHD_OK) return s;
+        const int row = src[p], G = n[row];
+        std::vector<T> rows((size_t)G * kRow);
+        if (G) {
+            CUDA_TRY(cudaMemcpyAsync(rows.data(), b.map[cur] + (size_t)row * prm.Gcap * kRow, sizeof(T) * G * kRow,
+                                     cudaMemcpyDeviceToHost, stream));
+            CUDA_TRY(cudaStreamSynchronize(stream));
+        }
+        const T ps = pending ? (T)prm.ps : T(1);
+        for (int j = 0; j < G; ++j) w[j] = (double)(rows[(size_t)j * kRow] * ps);
+        return SCPHD_OK;
+    }
+
+    scphd_status get_map_clouds(int p, double* xyz, double* om) override {
+        std::vector<int> src, n;
+        scphd_status s = host_rows(src, n);
+        if (s != SCPHD_OK) return s;
+        const int G = n[src[p]], P = prm.P, Ps = prm.Ps;
+        if (G == 0) return SCPHD_OK;
+        k_materialize<T><<<1, 256, 0, stream>>>(prm, b, cur, dump, nullptr, nullptr, nullptr, pending ? 1 : 0,
+                                                 pending_dt, pending_frame, sample_frame[cur], p);
+        LAUNCHED();
+        std::vector<T> h((size_t)G * 7 * Ps);
+        CUDA_TRY(cudaMemcpyAsync(h.data(), dump, sizeof(T) * h.size(), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        for (int j = 0; j < G; ++j)
+            for (int s2 = 0; s2 < P; ++s2) {
+                for (int a = 0; a < 6; ++a)
+                    if (xyz) xyz[((size_t)j * 6 + a) * P + s2] = (double)h[((size_t)j * 7 + a) * Ps + s2];
+                if (om) om[(size_t)j * P + s2] = (double)h[((size_t)j * 7 + 6) * Ps + s2];
+            }
+        return SCPHD_OK;
+    }
+
+    scphd_status get_mixture(int which, int p, double* out, int32_t* count) override {
+        int cnt = 0;
+        const T* base;
+        int width;
+        if (which == SCPHD_MIX_FITTED) {
+            CUDA_TRY(cudaMemcpyAsync(&cnt, fit_n + p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+            base = b.fit + (size_t)p * prm.Gcap * kRow;
+            width = 29;
+        } else if (which == SCPHD_MIX_MERGED) {
+            CUDA_TRY(cudaMemcpyAsync(&cnt, b.merged_n + p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+            base = b.merged + (size_t)p * prm.Scap * kRow;
+            width = 28;
+        } else {
+            return fail(SCPHD_ERR_INVALID, "unknown mixture selector");
+        }
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        if (count) *count = cnt;
+        if (!out || cnt == 0) return SCPHD_OK;
+        std::vector<T> rows((size_t)cnt * kRow);
+        CUDA_TRY(cudaMemcpyAsync(rows.data(), base, sizeof(T) * rows.size(), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        for (int i = 0; i < cnt; ++i)
+            for (int q = 0; q < width; ++q) out[(size_t)i * width + q] = (double)rows[(size_t)i * kRow + q];
+        return SCPHD_OK;
+    }
+
+    scphd_status get_normalizers(double* ell, double* ll) override {
+        if (ell && last_M > 0) {
+            std::vector<T> h((size_t)prm.N * prm.Mcap);
+            CUDA_TRY(cudaMemcpyAsync(h.data(), b.ell, sizeof(T) * h.size(), cudaMemcpyDeviceToHost, stream));
+            CUDA_TRY(cudaStreamSynchronize(stream));
+            for (int p = 0; p < prm.N; ++p)
+                for (int m = 0; m < last_M; ++m) ell[(size_t)p * last_M + m] = (double)h[(size_t)p * prm.Mcap + m];
+        }
+        if (ll) {
+            CUDA_TRY(cudaMemcpyAsync(ll, b.loglik, sizeof(double) * prm.N, cudaMemcpyDeviceToHost, stream));
+            CUDA_TRY(cudaStreamSynchronize(stream));
+        }
+        return SCPHD_OK;
+    }
+
+    scphd_status get_resample_indices(int32_t* idx) override {
+        CUDA_TRY(cudaMemcpyAsync(idx, b.resample_idx, sizeof(int) * prm.N, cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        return SCPHD_OK;
+    }
+
+    scphd_status set_state(const double* st, const double* lw, const int32_t* sizes, const double* w,
+                           const double* xyz, const double* om) override {
+        const int N = prm.N, G = prm.Gcap, P = prm.P, Ps = prm.Ps;
+        for (int p = 0; p < N; ++p)
+            if (sizes[p] < 0 || sizes[p] > G) return fail(SCPHD_ERR_CAPACITY, "map size exceeds max_gaussians");
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        std::vector<T> cl((size_t)N * G * 7 * Ps, T(0)), mp((size_t)N * G * kRow, T(0));
+        std::vector<int> ref((size_t)N * G, 0), n(N), src(N);
+        size_t g = 0;
+        for (int p = 0; p < N; ++p) {
+            n[p] = sizes[p];
+            src[p] = p;
+            for (int j = 0; j < sizes[p]; ++j, ++g) {
+                size_t r = (size_t)p * G + j;
+                mp[r * kRow] = (T)w[g];
+                ref[r] = (int)r;
+                for (int s2 = 0; s2 < P; ++s2) {
+                    for (int a = 0; a < 6; ++a) cl[(r * 7 + a) * Ps + s2] = (T)xyz[(g * 6 + a) * P + s2];
+                    cl[(r * 7 + 6) * Ps + s2] = (T)om[g * P + s2];
+                }
+            }
+        }
+        CUDA_TRY(cudaMemcpy(b.cloud[cur], cl.data(), sizeof(T) * cl.size(), cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(b.map[cur], mp.data(), sizeof(T) * mp.size(), cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(b.map_ref[cur], ref.data(), sizeof(int) * ref.size(), cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(b.map_n[cur], n.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(b.src, src.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(b.ext, st, sizeof(double) * 12 * N, cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(b.lw, lw, sizeof(double) * N, cudaMemcpyHostToDevice));
+        pending = false;
+        return SCPHD_OK;
+    }
+
+    scphd_status get_counters(int64_t* c) override {
+        unsigned long long h[8];
+        CUDA_TRY(cudaMemcpyAsync(h, b.counters, sizeof(h), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        for (int i = 0; i < 8; ++i) c[i] = (int64_t)h[i];
+        return SCPHD_OK;
+    }
+
+    scphd_status check() override {
+        std::vector<double> lw(prm.N);
+        CUDA_TRY(cudaMemcpyAsync(lw.data(), b.lw, sizeof(double) * prm.N, cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        for (double v : lw)
+            if (std::isnan(v)) return fail(SCPHD_ERR_NAN, "nan weight detected");
+        return SCPHD_OK;
+    }
+};
+
+scphd_status validate(const scphd_config* c) {
+    if (!c) return fail(SCPHD_ERR_INVALID, "null config");
+    if (c->n_parents < 1 || c->n_parents > (1 << 20)) return fail(SCPHD_ERR_INVALID, "n_parents out of range");
+    if (c->particles_per_feature < 1 || c->particles_per_feature > 256)
+        return fail(SCPHD_ERR_INVALID, "particles_per_feature must be in [1, 256]");
+    if (c->max_gaussians < 1) return fail(SCPHD_ERR_INVALID, "max_gaussians must be >= 1");
+    if (c->max_measurements < 1) return fail(SCPHD_ERR_INVALID, "max_measurements must be >= 1");
+    if (c->meas_dim != 2 && c->meas_dim != 3) return fail(SCPHD_ERR_INVALID, "meas_dim must be 2 or 3");
+    if (c->precision != SCPHD_FP32 && c->precision != SCPHD_FP64) return fail(SCPHD_ERR_INVALID, "bad precision");
+    if ((double)c->max_gaussians * c->max_measurements > 2e9) return fail(SCPHD_ERR_INVALID, "G x M too large");
+    if (c->baseline == 0 || c->fy == 0) return fail(SCPHD_ERR_INVALID, "baseline and fy must be non-zero");
+    if (!(c->min_separation > 0)) return fail(SCPHD_ERR_INVALID, "min_separation must be > 0");
+    if (!(c->min_weight > 0)) return fail(SCPHD_ERR_INVALID, "min_weight must be > 0");
+    return SCPHD_OK;
+}
+
+Params make_params(const scphd_config& c) {
+    Params p{};
+    p.N = c.n_parents;
+    p.P = c.particles_per_feature;
+    p.Gcap = c.max_gaussians;
+    p.Mcap = c.max_measurements;
+    p.Scap = c.max_survivors > 0 ? c.max_survivors : 4 * c.max_gaussians + c.max_measurements;
+    p.K = c.meas_dim;
+    p.Ps = round_up(c.particles_per_feature, c.precision == SCPHD_FP64 ? 4 : 8);
+    p.model.fx = c.fx; p.model.fy = c.fy; p.model.u0 = c.u0; p.model.v0 = c.v0;
+    p.model.B = c.baseline; p.model.pd = c.pd;
+    p.model.var[0] = c.std_u * c.std_u;
+    p.model.var[1] = c.std_v * c.std_v;
+    p.model.var[2] = c.std_d * c.std_d;
+    p.kappa = c.kappa; p.ps = c.ps; p.min_weight = c.min_weight; p.min_sep = c.min_separation;
+    p.min_neff = c.min_neff;
+    p.w0 = c.w0; p.d0 = c.d0; p.vu0 = c.vu0; p.vv0 = c.vv0; p.vd0 = c.vd0;
+    p.var_d0 = c.var_d0; p.var_vu0 = c.var_vu0; p.var_vv0 = c.var_vv0; p.var_vd0 = c.var_vd0;
+    for (int i = 0; i < 6; ++i) p.cam_std[i] = c.cam_std[i];
+    for (int i = 0; i < 3; ++i) p.feat_std[i] = c.feat_std[i];
+    for (int i = 0; i < 12; ++i) { p.prior_a[i] = c.prior_a[i]; p.prior_b[i] = c.prior_b[i]; }
+    p.key0 = (uint32_t)c.seed;
+    p.key1 = (uint32_t)(c.seed >> 32);
+    return p;
+}
+
+scphd_status stage_host(scphd_filter* f, const double* u, const double* v, const double* d, int32_t n) {
+    if (n < 0) return fail(SCPHD_ERR_INVALID, "negative measurement count");
+    if (n > f->prm.Mcap) return fail(SCPHD_ERR_CAPACITY, "more measurements than max_measurements");
+    if (n > 0 && (!u || !v)) return fail(SCPHD_ERR_INVALID, "null measurement array");
+    if (f->prm.K == 3 && n > 0 && !d) return fail(SCPHD_ERR_INVALID, "meas_dim 3 needs the disparity array");
+    if (n == 0) return SCPHD_OK;
+    for (int i = 0; i < n; ++i)
+        if (!std::isfinite(u[i]) || !std::isfinite(v[i]) || (f->prm.K == 3 && !std::isfinite(d[i])))
+            return fail(SCPHD_ERR_INVALID, "non-finite measurement");
+    CUDA_TRY(cudaEventSynchronize(f->stage_ev));   // previous copy out of the pinned buffer is done
+    std::memcpy(f->h_stage, u, sizeof(double) * n);
+    std::memcpy(f->h_stage + n, v, sizeof(double) * n);
+    if (d) std::memcpy(f->h_stage + 2 * n, d, sizeof(double) * n);
+    CUDA_TRY(cudaMemcpyAsync(f->d_stage, f->h_stage, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, f->stream));
+    CUDA_TRY(cudaEventRecord(f->stage_ev, f->stream));
+    return SCPHD_OK;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+void scphd_config_defaults(scphd_config* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->n_parents = 100;
+    c->particles_per_feature = 100;
+    c->max_gaussians = 256;
+    c->max_measurements = 64;
+    c->meas_dim = 2;
+    c->precision = SCPHD_FP64;
+    c->seed = 0x5C9D0000ull;
+    const double mean[12] = {0, -50, -3, 0, 0, 0, 0.3927, 0.1, 0, 0, 0, 0};
+    const double sd[12] = {0, 0, 3, 0, 0, 0, 0, 0.1, 0, 0, 0, 0};
+    for (int i = 0; i < 12; ++i) { c->prior_a[i] = mean[i] - sd[i]; c->prior_b[i] = mean[i] + sd[i]; }
+    const double cam[6] = {0, 0, 0.15, 0, 0.001, 0};
+    for (int i = 0; i < 6; ++i) c->cam_std[i] = cam[i];
+    c->feat_std[0] = 0.05; c->feat_std[1] = 0.05; c->feat_std[2] = 0.1;
+    c->fx = -895.6561; c->fy = -891.2656; c->u0 = 400; c->v0 = 300;
+    c->std_u = 5; c->std_v = 5; c->std_d = 1; c->pd = 0.95;
+    c->kappa = 10.0001 / (600.0 * 600.0);
+    c->baseline = 1;
+    c->ps = 0.9; c->min_weight = 1e-4; c->min_separation = 6.0; c->min_neff = 0.75;
+    c->w0 = 1e-6; c->d0 = 8; c->vu0 = 0; c->vv0 = 0; c->vd0 = 0;
+    c->var_d0 = 2; c->var_vu0 = 6; c->var_vv0 = 6; c->var_vd0 = 0.05;
+}
+
+scphd_status scphd_create(const scphd_config* cfg, scphd_filter** out) {
+    if (!out) return fail(SCPHD_ERR_INVALID, "null output handle");
+    *out = nullptr;
+    scphd_status s = validate(cfg);
+    if (s != SCPHD_OK) return s;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(SCPHD_ERR_NO_DEVICE, "no CUDA device");
+    if (cfg->device < 0 || cfg->device >= ndev) return fail(SCPHD_ERR_INVALID, "device ordinal out of range");
+    CUDA_TRY(cudaSetDevice(cfg->device));
+    scphd_filter* f = cfg->precision == SCPHD_FP64 ? static_cast<scphd_filter*>(new Filter<double>())
+                                                   : static_cast<scphd_filter*>(new Filter<float>());
+    f->cfg = *cfg;
+    f->prm = make_params(*cfg);
+    s = f->init();
+    if (s != SCPHD_OK) {
+        delete f;
+        return s;
+    }
+    *out = f;
+    return SCPHD_OK;
+}
+
+scphd_status scphd_destroy(scphd_filter* f) {
+    if (!f) return fail(SCPHD_ERR_INVALID, "null handle");
+    cudaSetDevice(f->cfg.device);
+    delete f;
+    return SCPHD_OK;
+}
+
+#define HANDLE(f)                                                  \
+    do {                                                           \
+        if (!(f)) return fail(SCPHD_ERR_INVALID, "null handle");   \
+        CUDA_TRY(cudaSetDevice((f)->cfg.device));                  \
+    } while (0)
+
+scphd_status scphd_predict(scphd_filter* f, double dt) {
+    HANDLE(f);
+    if (!std::isfinite(dt)) return fail(SCPHD_ERR_INVALID, "dt must be finite");
+    return f->predict(dt);
+}
+
+scphd_status scphd_update(scphd_filter* f, const double* u, const double* v, const double* d, int32_t n,
+                          int32_t fixed_camera) {
+    HANDLE(f);
+    scphd_status s = stage_host(f, u, v, d, n);
+    if (s != SCPHD_OK) return s;
+    return f->update_staged(n, fixed_camera ? 1 : 0);
+}
+
+scphd_status scphd_update_device(scphd_filter* f, const double* u, const double* v, const double* d, int32_t n,
+                                 int32_t fixed_camera) {
+    HANDLE(f);
+    if (n < 0) return fail(SCPHD_ERR_INVALID, "negative measurement count");
+    if (n > f->prm.Mcap) return fail(SCPHD_ERR_CAPACITY, "more measurements than max_measurements");
+    if (f->prm.K == 3 && n > 0 && !d) return fail(SCPHD_ERR_INVALID, "meas_dim 3 needs the disparity array");
+    if (n > 0) {
+        CUDA_TRY(cudaMemcpyAsync(f->d_stage, u, sizeof(double) * n, cudaMemcpyDeviceToDevice, f->stream));
+        CUDA_TRY(cudaMemcpyAsync(f->d_stage + n, v, sizeof(double) * n, cudaMemcpyDeviceToDevice, f->stream));
+        if (d) CUDA_TRY(cudaMemcpyAsync(f->d_stage + 2 * n, d, sizeof(double) * n, cudaMemcpyDeviceToDevice, f->stream));
+    }
+    return f->update_staged(n, fixed_camera ? 1 : 0);
+}
+
+scphd_status scphd_resample(scphd_filter* f, int32_t* resampled) {
+    HANDLE(f);
+    return f->resample(resampled, true);
+}
+
+scphd_status scphd_step(scphd_filter* f, double dt, const double* u, const double* v, const double* d, int32_t n,
+                        int32_t fixed_camera) {
+    HANDLE(f);
+    if (!std::isfinite(dt)) return fail(SCPHD_ERR_INVALID, "dt must be finite");
+    scphd_status s = stage_host(f, u, v, d, n);
+    if (s != SCPHD_OK) return s;
+    s = f->predict(dt);
+    if (s != SCPHD_OK) return s;
+    s = f->update_staged(n, fixed_camera ? 1 : 0);
+    if (s != SCPHD_OK) return s;
+    return f->resample(nullptr, false);
+}
+
+scphd_status scphd_check(scphd_filter* f) {
+    HANDLE(f);
+    return f->check();
+}
+
+scphd_status scphd_synchronize(scphd_filter* f) {
+    HANDLE(f);
+    CUDA_TRY(cudaStreamSynchronize(f->stream));
+    return SCPHD_OK;
+}
+
+scphd_status scphd_get_particles(scphd_filter* f, double* states, double* log_weights) {
+    HANDLE(f);
+    return f->get_particles(states, log_weights);
+}
+
+scphd_status scphd_get_map_sizes(scphd_filter* f, int32_t* sizes) {
+    HANDLE(f);
+    if (!sizes) return fail(SCPHD_ERR_INVALID, "null output");
+    return f->get_map_sizes(sizes);
+}
+
+scphd_status scphd_get_map_weights(scphd_filter* f, int32_t p, double* weights) {
+    HANDLE(f);
+    if (p < 0 || p >= f->prm.N || !weights) return fail(SCPHD_ERR_INVALID, "bad parent index or output");
+    return f->get_map_weights(p, weights);
+}
+
+scphd_status scphd_get_map_clouds(scphd_filter* f, int32_t p, double* xyz, double* omega) {
+    HANDLE(f);
+    if (p < 0 || p >= f->prm.N) return fail(SCPHD_ERR_INVALID, "bad parent index");
+    return f->get_map_clouds(p, xyz, omega);
+}
+
+scphd_status scphd_get_mixture(scphd_filter* f, int32_t which, int32_t p, double* out, int32_t* count) {
+    HANDLE(f);
+    if (p < 0 || p >= f->prm.N) return fail(SCPHD_ERR_INVALID, "bad parent index");
+    return f->get_mixture(which, p, out, count);
+}
+
+scphd_status scphd_get_normalizers(scphd_filter* f, double* ell, double* loglik) {
+    HANDLE(f);
+    return f->get_normalizers(ell, loglik);
+}
+
+scphd_status scphd_get_resample_indices(scphd_filter* f, int32_t* idx) {
+    HANDLE(f);
+    if (!idx) return fail(SCPHD_ERR_INVALID, "null output");
+    return f->get_resample_indices(idx);
+}
+
+scphd_status scphd_set_state(scphd_filter* f, const double* states, const double* log_weights, const int32_t* sizes,
+                             const double* weights, const double* clouds, const double* omega) {
+    HANDLE(f);
+    if (!states || !log_weights || !sizes) return fail(SCPHD_ERR_INVALID, "null state array");
+    return f->set_state(states, log_weights, sizes, weights, clouds, omega);
+}
+
+scphd_status scphd_get_counters(scphd_filter* f, int64_t counters[8]) {
+    HANDLE(f);
+    if (!counters) return fail(SCPHD_ERR_INVALID, "null output");
+    return f->get_counters(counters);
+}
+
+scphd_status scphd_merge_components(const double* comps, const uint8_t* flags, int32_t n, double min_separation,
+                                    int32_t precision, double* merged, int32_t* n_out, int32_t* member_of) {
+    if (n < 0 || (n > 0 && (!comps || !flags || !merged || !n_out))) return fail(SCPHD_ERR_INVALID, "bad arguments");
+    if (n > 2048) return fail(SCPHD_ERR_CAPACITY, "at most 2048 components");
+    if (!(min_separation > 0)) return fail(SCPHD_ERR_INVALID, "min_separation must be > 0");
+    if (n_out) *n_out = 0;
+    if (n == 0) return SCPHD_OK;
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    auto run = [&](auto tag) -> scphd_status {
+        using T = decltype(tag);
+        std::vector<T> rows((size_t)n * kRow, T(0));
+        for (int i = 0; i < n; ++i)
+            for (int q = 0; q < 28; ++q) rows[(size_t)i * kRow + q] = (T)comps[(size_t)i * 28 + q];
+        T *d_rows = nullptr, *d_out = nullptr;
+        uint8_t* d_flags = nullptr;
+        int* d_n = nullptr;
+        int* d_mem = nullptr;
+        size_t smem = (size_t)(2 * n + 2) * (sizeof(T) + 8) + (size_t)(6 * n + 6) * sizeof(T) + n + 64;
+        scphd_status st = SCPHD_OK;
+        std::vector<T> out((size_t)n * kRow);
+        int nout = 0;
+        std::vector<int> mem(n, -1);
+        do {
+            if (cudaMalloc(&d_rows, sizeof(T) * rows.size()) != cudaSuccess ||
+                cudaMalloc(&d_out, sizeof(T) * rows.size()) != cudaSuccess ||
+                cudaMalloc(&d_flags, n) != cudaSuccess || cudaMalloc(&d_n, sizeof(int)) != cudaSuccess ||
+                cudaMalloc(&d_mem, sizeof(int) * n) != cudaSuccess) {
+                st = fail(SCPHD_ERR_CUDA, "allocation for merge_components failed");
+                break;
+            }
+            cudaMemcpy(d_rows, rows.data(), sizeof(T) * rows.size(), cudaMemcpyHostToDevice);
+            cudaMemcpy(d_flags, flags, n, cudaMemcpyHostToDevice);
+            cudaMemset(d_mem, 0xff, sizeof(int) * n);
+            cudaFuncSetAttribute(k_merge_list<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            k_merge_list<T><<<1, 128, smem>>>(d_rows, d_flags, n, (T)min_separation, d_out, d_n, d_mem);
+            g_launches.fetch_add(1, std::memory_order_relaxed);
+            cudaError_t e = cudaDeviceSynchronize();
+            if (e != cudaSuccess) {
+                st = fail(SCPHD_ERR_CUDA, std::string("k_merge_list: ") + cudaGetErrorString(e));
+                break;
+            }
+            cudaMemcpy(&nout, d_n, sizeof(int), cudaMemcpyDeviceToHost);
+            cudaMemcpy(out.data(), d_out, sizeof(T) * out.size(), cudaMemcpyDeviceToHost);
+            cudaMemcpy(mem.data(), d_mem, sizeof(int) * n, cudaMemcpyDeviceToHost);
+        } while (0);
+        cudaFree(d_rows); cudaFree(d_out); cudaFree(d_flags); cudaFree(d_n); cudaFree(d_mem);
+        if (st != SCPHD_OK) return st;
+        *n_out = nout;
+        for (int i = 0; i < nout; ++i)
+            for (int q = 0; q < 28; ++q) merged[(size_t)i * 28 + q] = (double)out[(size_t)i * kRow + q];
+        if (member_of)
+            for (int i = 0; i < n; ++i) member_of[i] = mem[i];
+        return SCPHD_OK;
+    };
+    (void)dev;
+    return precision == SCPHD_FP64 ? run(double()) : run(float());
+}
+
+scphd_status scphd_systematic_resample(const double* weights, int32_t n, double u01v, int32_t* idx) {
+    if (n < 1 || n > 16 * 1024 * 1024 || !weights || !idx) return fail(SCPHD_ERR_INVALID, "bad arguments");
+    Params prm{};
+    prm.N = n;
+    prm.min_neff = 2.0;
+    double *d_lw = nullptr, *d_ext = nullptr, *d_ext_tmp = nullptr, *d_cum = nullptr, *d_scal = nullptr;
+    int *d_src = nullptr, *d_src_tmp = nullptr, *d_flags = nullptr, *d_idx = nullptr;
+    std::vector<double> lw(n);
+    for (int i = 0; i < n; ++i) lw[i] = std::log(weights[i]);
+    scphd_status st = SCPHD_OK;
+    do {
+        if (cudaMalloc(&d_lw, 8 * n) || cudaMalloc(&d_ext, 96 * (size_t)n) || cudaMalloc(&d_ext_tmp, 96 * (size_t)n) ||
+            cudaMalloc(&d_cum, 8 * n) || cudaMalloc(&d_scal, 32) || cudaMalloc(&d_src, 4 * n) ||
+            cudaMalloc(&d_src_tmp, 4 * n) || cudaMalloc(&d_flags, 16) || cudaMalloc(&d_idx, 4 * n)) {
+            st = fail(SCPHD_ERR_CUDA, "allocation for systematic_resample failed");
+            break;
+        }
+        cudaMemcpy(d_lw, lw.data(), 8 * n, cudaMemcpyHostToDevice);
+        cudaMemset(d_ext, 0, 96 * (size_t)n);
+        cudaMemset(d_src, 0, 4 * n);
+        k_resample<<<1, 1024>>>(prm, d_lw, d_ext, d_ext_tmp, d_src, d_src_tmp, d_cum, d_scal, d_flags, d_idx, 0, 1,
+                                u01v, nullptr);
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) {
+            st = fail(SCPHD_ERR_CUDA, std::string("k_resample: ") + cudaGetErrorString(e));
+            break;
+        }
+        cudaMemcpy(idx, d_idx, 4 * n, cudaMemcpyDeviceToHost);
+    } while (0);
+    cudaFree(d_lw); cudaFree(d_ext); cudaFree(d_ext_tmp); cudaFree(d_cum); cudaFree(d_scal);
+    cudaFree(d_src); cudaFree(d_src_tmp); cudaFree(d_flags); cudaFree(d_idx);
+    return st;
+}
+
+const char* scphd_last_error(void) { return g_err.c_str(); }
+
+int64_t scphd_kernel_launches(void) { return g_launches.load(); }
+
+}  // extern "C"

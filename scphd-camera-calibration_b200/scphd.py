@@ -1,0 +1,354 @@
+"""Python binding of the B200 SC-PHD calibration filter (ctypes over the C ABI).
+
+`SCPHDCameraCalibration` mirrors the step API of the reference class of the same
+name (src/scphdcameracalibration.cuh:29-44): predict(dt), update(u, v,
+fixed_camera) -- with an optional disparity vector d for (u,v,d) measurements --
+resample(), checkStuff() and the particle/mixture dumps of writeMat().  Errors
+raise ScphdError with the library's message; there is no CPU fallback: if the
+CUDA library cannot be loaded, constructing a filter fails.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "csrc", "libscphd_b200.so")
+
+SCPHD_FP32 = 0
+SCPHD_FP64 = 1
+SCPHD_MIX_FITTED = 0
+SCPHD_MIX_MERGED = 1
+
+_STATUS = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "CAPACITY", 4: "NAN", 5: "NO_DEVICE"}
+
+
+class ScphdError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"scphd {_STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class ScphdConfig(ctypes.Structure):
+    """Mirror of `scphd_config` in include/scphd.h (field order and types)."""
+
+    _fields_ = [
+        ("n_parents", ctypes.c_int32),
+        ("particles_per_feature", ctypes.c_int32),
+        ("max_gaussians", ctypes.c_int32),
+        ("max_measurements", ctypes.c_int32),
+        ("meas_dim", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("max_survivors", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+        ("seed", ctypes.c_uint64),
+        ("prior_a", ctypes.c_double * 12),
+        ("prior_b", ctypes.c_double * 12),
+        ("cam_std", ctypes.c_double * 6),
+        ("feat_std", ctypes.c_double * 3),
+        ("fx", ctypes.c_double),
+        ("fy", ctypes.c_double),
+        ("u0", ctypes.c_double),
+        ("v0", ctypes.c_double),
+        ("std_u", ctypes.c_double),
+        ("std_v", ctypes.c_double),
+        ("std_d", ctypes.c_double),
+        ("pd", ctypes.c_double),
+        ("kappa", ctypes.c_double),
+        ("baseline", ctypes.c_double),
+        ("ps", ctypes.c_double),
+        ("min_weight", ctypes.c_double),
+        ("min_separation", ctypes.c_double),
+        ("min_neff", ctypes.c_double),
+        ("w0", ctypes.c_double),
+        ("d0", ctypes.c_double),
+        ("vu0", ctypes.c_double),
+        ("vv0", ctypes.c_double),
+        ("vd0", ctypes.c_double),
+        ("var_d0", ctypes.c_double),
+        ("var_vu0", ctypes.c_double),
+        ("var_vv0", ctypes.c_double),
+        ("var_vd0", ctypes.c_double),
+    ]
+
+    def copy(self) -> "ScphdConfig":
+        c = ScphdConfig()
+        ctypes.pointer(c)[0] = self
+        return c
+
+    def as_dict(self) -> dict:
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            out[name] = list(v) if isinstance(v, ctypes.Array) else v
+        return out
+
+
+def reference_defaults() -> ScphdConfig:
+    """The values of the reference's config/calibration.cfg, read the way its code
+    reads them (the shipped {mean,std} prior becomes the box mean +- max(std, 0)),
+    meas_dim 2, baseline 1, kappa = lambda / (2 v0)^2 with lambda = 10.0001
+    (src/disparitymeasurementmodel.cu:157-162)."""
+    c = ScphdConfig()
+    c.n_parents = 100
+    c.particles_per_feature = 100
+    c.max_gaussians = 256
+    c.max_measurements = 64
+    c.meas_dim = 2
+    c.precision = SCPHD_FP64
+    c.max_survivors = 0
+    c.device = 0
+    c.seed = 0x5C9D0000
+    mean = [0.0, -50.0, -3.0, 0.0, 0.0, 0.0, 0.3927, 0.1, 0.0, 0.0, 0.0, 0.0]
+    std = [0.0, 0.0, 3.0, 0.0, 0.0, 0.0, 0.0, 0.1, 0.0, 0.0, 0.0, 0.0]
+    for i in range(12):
+        c.prior_a[i] = mean[i] - std[i]
+        c.prior_b[i] = mean[i] + std[i]
+    for i, v in enumerate([0.0, 0.0, 0.15, 0.0, 0.001, 0.0]):
+        c.cam_std[i] = v
+    for i, v in enumerate([0.05, 0.05, 0.1]):
+        c.feat_std[i] = v
+    c.fx, c.fy, c.u0, c.v0 = -895.6561, -891.2656, 400.0, 300.0
+    c.std_u = c.std_v = 5.0
+    c.std_d = 1.0
+    c.pd = 0.95
+    c.kappa = 10.0001 / (2 * 300.0) ** 2
+    c.baseline = 1.0
+    c.ps = 0.9
+    c.min_weight = 0.0001
+    c.min_separation = 6.0
+    c.min_neff = 0.75
+    c.w0, c.d0, c.vu0, c.vv0, c.vd0 = 0.000001, 8.0, 0.0, 0.0, 0.0
+    c.var_d0, c.var_vu0, c.var_vv0, c.var_vd0 = 2.0, 6.0, 6.0, 0.05
+    return c
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load the CUDA library.  Raises if it is missing: there is no fallback."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ScphdError(5, f"CUDA library not built: {path} (run __graft_entry__.build())")
+    lib = ctypes.CDLL(path)
+    P = ctypes.POINTER
+    d, i32, i64, u8 = ctypes.c_double, ctypes.c_int32, ctypes.c_int64, ctypes.c_uint8
+    vp = ctypes.c_void_p
+    sigs = {
+        "scphd_config_defaults": (None, [P(ScphdConfig)]),
+        "scphd_create": (i32, [P(ScphdConfig), P(vp)]),
+        "scphd_destroy": (i32, [vp]),
+        "scphd_predict": (i32, [vp, d]),
+        "scphd_update": (i32, [vp, P(d), P(d), P(d), i32, i32]),
+        "scphd_update_device": (i32, [vp, vp, vp, vp, i32, i32]),
+        "scphd_resample": (i32, [vp, P(i32)]),
+        "scphd_step": (i32, [vp, d, P(d), P(d), P(d), i32, i32]),
+        "scphd_check": (i32, [vp]),
+        "scphd_synchronize": (i32, [vp]),
+        "scphd_get_particles": (i32, [vp, P(d), P(d)]),
+        "scphd_get_map_sizes": (i32, [vp, P(i32)]),
+        "scphd_get_map_weights": (i32, [vp, i32, P(d)]),
+        "scphd_get_map_clouds": (i32, [vp, i32, P(d), P(d)]),
+        "scphd_get_mixture": (i32, [vp, i32, i32, P(d), P(i32)]),
+        "scphd_get_normalizers": (i32, [vp, P(d), P(d)]),
+        "scphd_get_resample_indices": (i32, [vp, P(i32)]),
+        "scphd_set_state": (i32, [vp, P(d), P(d), P(i32), P(d), P(d), P(d)]),
+        "scphd_get_counters": (i32, [vp, P(i64)]),
+        "scphd_merge_components": (i32, [P(d), P(u8), i32, d, i32, P(d), P(i32), P(i32)]),
+        "scphd_systematic_resample": (i32, [P(d), i32, d, P(i32)]),
+        "scphd_last_error": (ctypes.c_char_p, []),
+        "scphd_kernel_launches": (i64, []),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        msg = _lib.scphd_last_error() if _lib is not None else b""
+        raise ScphdError(status, (msg or b"").decode(errors="replace"))
+
+
+def _dptr(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _iptr(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+def _f64(x) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+
+
+def kernel_launches() -> int:
+    return int(load_library().scphd_kernel_launches())
+
+
+class SCPHDCameraCalibration:
+    """One SC-PHD calibration filter on one GPU (the reference's class, re-hosted)."""
+
+    def __init__(self, config: ScphdConfig):
+        self._lib = load_library()
+        self.config = config.copy()
+        h = ctypes.c_void_p()
+        _check(self._lib.scphd_create(ctypes.byref(self.config), ctypes.byref(h)))
+        self._h = h
+
+    # -- lifecycle
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            _check(self._lib.scphd_destroy(self._h))
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def n_parents(self) -> int:
+        return int(self.config.n_parents)
+
+    # -- the reference's step API
+    def predict(self, dt: float) -> None:
+        _check(self._lib.scphd_predict(self._h, float(dt)))
+
+    def update(self, u: Sequence[float], v: Sequence[float], fixed_camera: bool = False,
+               d: Optional[Sequence[float]] = None) -> None:
+        u, v = _f64(u), _f64(v)
+        dd = _f64(d) if d is not None else None
+        if u.shape != v.shape or (dd is not None and dd.shape != u.shape):
+            raise ScphdError(1, "u, v (and d) must have the same length")
+        _check(self._lib.scphd_update(self._h, _dptr(u), _dptr(v), _dptr(dd), int(u.size),
+                                      int(bool(fixed_camera))))
+
+    def update_device(self, u_ptr: int, v_ptr: int, d_ptr: Optional[int], n: int,
+                      fixed_camera: bool = False) -> None:
+        """update() with measurement vectors already resident in device memory
+        (FP64 device pointers, e.g. torch tensors' data_ptr())."""
+        _check(self._lib.scphd_update_device(self._h, ctypes.c_void_p(u_ptr), ctypes.c_void_p(v_ptr),
+                                             ctypes.c_void_p(d_ptr) if d_ptr else None, int(n),
+                                             int(bool(fixed_camera))))
+
+    def resample(self) -> bool:
+        r = ctypes.c_int32(0)
+        _check(self._lib.scphd_resample(self._h, ctypes.byref(r)))
+        return bool(r.value)
+
+    def step(self, dt: float, u, v, fixed_camera: bool = False, d=None) -> None:
+        u, v = _f64(u), _f64(v)
+        dd = _f64(d) if d is not None else None
+        _check(self._lib.scphd_step(self._h, float(dt), _dptr(u), _dptr(v), _dptr(dd),
+                                    int(u.size), int(bool(fixed_camera))))
+
+    def checkStuff(self) -> None:
+        _check(self._lib.scphd_check(self._h))
+
+    check_stuff = checkStuff
+
+    def synchronize(self) -> None:
+        _check(self._lib.scphd_synchronize(self._h))
+
+    # -- state dumps (writeMat's particle / mixture content)
+    def particles(self):
+        n = self.n_parents
+        st = np.zeros((n, 12), np.float64)
+        lw = np.zeros(n, np.float64)
+        _check(self._lib.scphd_get_particles(self._h, _dptr(st), _dptr(lw)))
+        return st, lw
+
+    def map_sizes(self) -> np.ndarray:
+        s = np.zeros(self.n_parents, np.int32)
+        _check(self._lib.scphd_get_map_sizes(self._h, _iptr(s)))
+        return s
+
+    def map_weights(self, p: int) -> np.ndarray:
+        n = int(self.map_sizes()[p])
+        w = np.zeros(n, np.float64)
+        _check(self._lib.scphd_get_map_weights(self._h, int(p), _dptr(w)))
+        return w
+
+    def map_clouds(self, p: int):
+        n = int(self.map_sizes()[p])
+        P = int(self.config.particles_per_feature)
+        x = np.zeros((n, 6, P), np.float64)
+        om = np.zeros((n, P), np.float64)
+        _check(self._lib.scphd_get_map_clouds(self._h, int(p), _dptr(x), _dptr(om)))
+        return x, om
+
+    def mixture(self, which: int, p: int) -> np.ndarray:
+        cnt = ctypes.c_int32(0)
+        _check(self._lib.scphd_get_mixture(self._h, int(which), int(p), None, ctypes.byref(cnt)))
+        width = 29 if which == SCPHD_MIX_FITTED else 28
+        out = np.zeros((cnt.value, width), np.float64)
+        _check(self._lib.scphd_get_mixture(self._h, int(which), int(p), _dptr(out), ctypes.byref(cnt)))
+        return out
+
+    def normalizers(self, n_meas: int):
+        ell = np.zeros((self.n_parents, n_meas), np.float64)
+        ll = np.zeros(self.n_parents, np.float64)
+        _check(self._lib.scphd_get_normalizers(self._h, _dptr(ell), _dptr(ll)))
+        return ell, ll
+
+    def resample_indices(self) -> np.ndarray:
+        idx = np.zeros(self.n_parents, np.int32)
+        _check(self._lib.scphd_get_resample_indices(self._h, _iptr(idx)))
+        return idx
+
+    def counters(self) -> np.ndarray:
+        c = np.zeros(8, np.int64)
+        _check(self._lib.scphd_get_counters(self._h, c.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
+        return c
+
+    def set_state(self, states, log_weights, sizes, weights, clouds, omega) -> None:
+        states, log_weights = _f64(states), _f64(log_weights)
+        sizes = np.ascontiguousarray(np.asarray(sizes, np.int32))
+        weights, clouds, omega = _f64(weights), _f64(clouds), _f64(omega)
+        _check(self._lib.scphd_set_state(self._h, _dptr(states), _dptr(log_weights), _iptr(sizes),
+                                         _dptr(weights), _dptr(clouds), _dptr(omega)))
+
+
+def merge_components(comps: np.ndarray, flags: np.ndarray, min_separation: float,
+                     precision: int = SCPHD_FP64):
+    """Device greedy merge of one component list (rows of 28); see include/scphd.h."""
+    lib = load_library()
+    comps = _f64(comps).reshape(-1, 28)
+    n = comps.shape[0]
+    fl = np.ascontiguousarray(np.asarray(flags, np.uint8))
+    out = np.zeros((max(n, 1), 28), np.float64)
+    n_out = ctypes.c_int32(0)
+    mem = np.zeros(max(n, 1), np.int32)
+    _check(lib.scphd_merge_components(_dptr(comps), fl.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), n,
+                                      float(min_separation), int(precision), _dptr(out),
+                                      ctypes.byref(n_out), _iptr(mem)))
+    return out[: n_out.value], mem[:n]
+
+
+def systematic_resample(weights: np.ndarray, u01: float) -> np.ndarray:
+    lib = load_library()
+    w = _f64(weights)
+    idx = np.zeros(w.size, np.int32)
+    _check(lib.scphd_systematic_resample(_dptr(w), int(w.size), float(u01), _iptr(idx)))
+    return idx

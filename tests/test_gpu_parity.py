@@ -1,0 +1,156 @@
+"""Device path vs the FP64 oracle, frame by frame, through the C ABI.
+
+FP64 device mode: parent states, log-weights, map sizes, fitted and merged
+mixtures, normalisers and resampling indices against the oracle on the same
+seeded scenes and random streams.  Counts and resampling indices must match
+exactly; floating point within the tolerances stated below.
+"""
+import numpy as np
+import pytest
+
+from conftest import gpu_available
+
+pytestmark = pytest.mark.gpu
+
+# FP64 device arithmetic differs from the oracle only in operation order and in
+# CUDA's vs glibc's log/sin/cos (<= 2 ulp): relative tolerances for FP64 mode
+RT_STATE = 1e-9      # parent states (FP64 path in both modes)
+RT_LW = 1e-7         # parent log-weights (sum of ~M log-normalisers)
+RT_MIX = 1e-6        # means/covariances of fitted and merged mixtures
+AT_MIX = 1e-7
+
+
+def _need_gpu():
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+
+
+def _pair(pkg, orc, cfg):
+    return pkg.SCPHDCameraCalibration(cfg), orc.Oracle(cfg)
+
+
+def _compare_frame(gpu, ref, M, k, strict=True):
+    st_g, lw_g = gpu.particles()
+    st_r, lw_r = ref.particles()
+    np.testing.assert_allclose(st_g, st_r, rtol=RT_STATE, atol=1e-9, err_msg=f"frame {k} states")
+    np.testing.assert_allclose(lw_g, lw_r, rtol=RT_LW, atol=1e-7, err_msg=f"frame {k} log-weights")
+    ng, nr = gpu.map_sizes(), ref.map_sizes()
+    assert np.array_equal(ng, nr), f"frame {k} map sizes {ng[:8]} vs {nr[:8]}"
+    if M > 0:
+        eg, llg = gpu.normalizers(M)
+        er, llr = ref.normalizers(M)
+        np.testing.assert_allclose(eg, er, rtol=1e-9, atol=1e-9, err_msg=f"frame {k} normalisers")
+        np.testing.assert_allclose(llg, llr, rtol=1e-9, atol=1e-7, err_msg=f"frame {k} loglik")
+    for p in range(0, gpu.n_parents, max(1, gpu.n_parents // 4)):
+        fg, fr = gpu.mixture(0, p), ref.fitted(p)
+        assert fg.shape == fr.shape, f"frame {k} parent {p} fitted count"
+        live = fr[:, 1] > 0   # fits of all-out-of-view clouds are placeholders in both
+        np.testing.assert_allclose(fg[live], fr[live], rtol=RT_MIX, atol=AT_MIX,
+                                   err_msg=f"frame {k} parent {p} fitted")
+        mg, mr = gpu.mixture(1, p), ref.merged(p)
+        assert mg.shape == mr.shape, f"frame {k} parent {p} merged count {mg.shape} vs {mr.shape}"
+        np.testing.assert_allclose(mg, mr, rtol=RT_MIX, atol=AT_MIX, err_msg=f"frame {k} parent {p} merged")
+
+
+@pytest.mark.parametrize("meas_dim", [3, 2])
+def test_fp64_frames_match_oracle(pkg, orc, meas_dim):
+    _need_gpu()
+    sc = pkg.scene.make_scene(n_landmarks=20, n_frames=8, clutter_rate=4.0, seed=pkg.scene.scene_seed(0, 11))
+    cfg = pkg.scene.filter_config(n_parents=48, max_gaussians=160, max_meas=96, clutter_rate=4.0,
+                                  precision=pkg.SCPHD_FP64, calib=sc.calib, seed=11, particles_per_feature=48,
+                                  meas_dim=meas_dim)
+    gpu, ref = _pair(pkg, orc, cfg)
+    for k in range(sc.n_frames):
+        z = sc.frames[k]
+        for f in (gpu, ref):
+            f.predict(pkg.scene.DT)
+            f.update(z[:, 0], z[:, 1], fixed_camera=sc.fixed[k], d=z[:, 2] if meas_dim == 3 else None)
+        _compare_frame(gpu, ref, z.shape[0], k)
+        rg, rr = gpu.resample(), ref.resample()
+        assert rg == rr, f"frame {k} resample decision"
+        if rr:
+            assert np.array_equal(gpu.resample_indices(), ref.resample_indices()), f"frame {k} resample idx"
+    c = gpu.counters()
+    assert c[0] == 0 and c[1] == 0, f"capacity hit in a parity scene: {c}"
+
+
+def test_reference_fixture_frames(pkg, orc):
+    """The reference's own measurement frames (data/disparity_sim.mat, committed as
+    tests/golden/disparity_sim_frames.npz) with its shipped model parameters."""
+    _need_gpu()
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "disparity_sim_frames.npz"))
+    cfg = pkg.reference_defaults()
+    cfg.n_parents = 40
+    cfg.particles_per_feature = 64
+    cfg.max_gaussians = 256
+    cfg.max_measurements = 64
+    gpu, ref = _pair(pkg, orc, cfg)
+    for k in range(6):
+        Z = g["Z1_%d" % k] if k % 2 == 0 else g["Z2_%d" % k]
+        for f in (gpu, ref):
+            f.predict(0.5)
+            f.update(Z[0], Z[1], fixed_camera=(k % 2 == 0))
+        _compare_frame(gpu, ref, Z.shape[1], k)
+        assert gpu.resample() == ref.resample()
+
+
+def test_merge_decisions_identical_inputs(pkg, orc):
+    """Greedy merge on identical component lists: counts, membership exact."""
+    _need_gpu()
+    rng = np.random.default_rng(5)
+    for trial in range(6):
+        n = int(rng.integers(5, 300))
+        comps = np.zeros((n, 28))
+        centers = rng.uniform(0, 100, (max(1, n // 4), 6))
+        for i in range(n):
+            c = centers[rng.integers(len(centers))]
+            A = rng.normal(0, 1, (6, 6)) * 0.5
+            C = A @ A.T + np.diag(rng.uniform(0.5, 3, 6))
+            comps[i, 0] = rng.choice([rng.uniform(1e-3, 1), 0.25])   # exact ties too
+            comps[i, 1:7] = c + rng.normal(0, 1.0, 6)
+            comps[i, 7:] = [C[a, b] for a in range(6) for b in range(a + 1)]
+        flags = (rng.uniform(size=n) < 0.1).astype(np.uint8)
+        mo, memo = orc.merge(comps, flags, 6.0)
+        for prec in (pkg.SCPHD_FP64, pkg.SCPHD_FP32):
+            if prec == pkg.SCPHD_FP32:
+                comps32 = comps.astype(np.float32).astype(np.float64)
+                mo, memo = orc.merge(comps32, flags, 6.0)
+                mg, memg = pkg.merge_components(comps32, flags, 6.0, prec)
+                tol = dict(rtol=2e-4, atol=2e-4)
+            else:
+                mg, memg = pkg.merge_components(comps, flags, 6.0, prec)
+                tol = dict(rtol=1e-10, atol=1e-10)
+            assert mg.shape == mo.shape, f"trial {trial} prec {prec} count"
+            assert np.array_equal(memg, memo), f"trial {trial} prec {prec} membership"
+            np.testing.assert_allclose(mg, mo, **tol)
+
+
+def test_systematic_resample_identical_weights(pkg, orc):
+    _need_gpu()
+    rng = np.random.default_rng(9)
+    for n in (1, 7, 256, 1000, 4096, 16384):
+        w = rng.exponential(size=n) ** 3
+        w /= w.sum()
+        for u in (0.0001, 0.37, 0.9999):
+            a = pkg.systematic_resample(w, u)
+            b = orc.systematic(w, u)
+            assert np.array_equal(a, b), f"n={n} u={u}"
+
+
+def test_capacity_and_argument_errors(pkg):
+    _need_gpu()
+    cfg = pkg.reference_defaults()
+    cfg.n_parents = 8
+    cfg.max_measurements = 4
+    f = pkg.SCPHDCameraCalibration(cfg)
+    f.predict(0.5)
+    with pytest.raises(pkg.ScphdError) as e:
+        f.update(np.zeros(5), np.zeros(5))
+    assert e.value.status == 3
+    f.update(np.array([10.0]), np.array([20.0]))
+    f.update(np.zeros(0), np.zeros(0))   # empty frame is legal
+    bad = cfg.copy()
+    bad.meas_dim = 4
+    with pytest.raises(pkg.ScphdError):
+        pkg.SCPHDCameraCalibration(bad)

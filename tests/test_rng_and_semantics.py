@@ -1,0 +1,148 @@
+"""Random streams, argmax tie order, greedy merge and systematic resampling of the
+oracle, and the recurrence-level invariants the device path must share."""
+import numpy as np
+
+
+def test_philox_known_answers(orc):
+    # Random123 known-answer vectors for Philox4x32-10
+    assert orc.philox([0, 0, 0, 0], [0, 0]) == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+    assert orc.philox([0xFFFFFFFF] * 4, [0xFFFFFFFF] * 2) == [0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD]
+    assert orc.philox([0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344], [0xA4093822, 0x299F31D0]) == \
+        [0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]
+
+
+def test_normals_are_standard(orc):
+    z = np.concatenate([orc.normals4(123, s, 0, 0, orc.ctr_word3(5, orc.STAGE_SAMPLE, 0)) for s in range(20000)])
+    assert abs(z.mean()) < 0.02 and abs(z.std() - 1) < 0.02
+    # distinct stages and frames give distinct streams
+    a = orc.normals4(123, 0, 0, 0, orc.ctr_word3(5, orc.STAGE_SAMPLE, 0))
+    b = orc.normals4(123, 0, 0, 0, orc.ctr_word3(5, orc.STAGE_FEAT, 0))
+    c = orc.normals4(123, 0, 0, 0, orc.ctr_word3(6, orc.STAGE_SAMPLE, 0))
+    assert not np.allclose(a, b) and not np.allclose(a, c)
+
+
+def _bitrev8(t):
+    return int("{:08b}".format(t)[::-1], 2)
+
+
+def test_tie_key_reproduces_block_argmax():
+    """Simulate phdUpdateMergeKernel's argmax (src/kernels.cu:704-739) on equal weights:
+    256 threads, strided scan keeping the earliest, then the shared-memory tree."""
+    import sys
+    sys.path.insert(0, __file__.rsplit("/tests/", 1)[0])
+    from oracle import oracle as orc
+    rng = np.random.default_rng(0)
+    for trial in range(200):
+        n = int(rng.integers(1, 900))
+        w = rng.choice([0.5, 0.25, 0.125], size=n)
+        flagged = rng.uniform(size=n) < 0.3
+        # reference simulation
+        sdata = [-1] * 256
+        for base in range(0, n, 256):
+            for tid in range(256):
+                i = base + tid
+                if i < n and not flagged[i]:
+                    if sdata[tid] == -1 or w[sdata[tid]] < w[i]:
+                        sdata[tid] = i
+        s = 128
+        while s > 0:
+            for tid in range(s):
+                if sdata[tid] == -1:
+                    sdata[tid] = sdata[tid + s]
+                elif sdata[tid + s] >= 0 and w[sdata[tid]] < w[sdata[tid + s]]:
+                    sdata[tid] = sdata[tid + s]
+            s //= 2
+        want = sdata[0]
+        # oracle order
+        cand = [i for i in range(n) if not flagged[i]]
+        got = min(cand, key=lambda i: (-w[i], orc.tie_key(i))) if cand else -1
+        assert got == want, (trial, got, want)
+
+
+def _comp(mean, cov_diag, w):
+    c = np.zeros(28)
+    c[0] = w
+    c[1:7] = mean
+    C = np.diag(cov_diag)
+    c[7:] = [C[a, b] for a in range(6) for b in range(a + 1)]
+    return c
+
+
+def test_merge_moment_matching(orc):
+    a = _comp([0, 0, 0, 0, 0, 0], [1] * 6, 0.6)
+    b = _comp([0.5, 0, 0, 0, 0, 0], [1] * 6, 0.4)
+    far = _comp([50, 0, 0, 0, 0, 0], [1] * 6, 0.3)
+    out, mem = orc.merge(np.stack([a, b, far]), np.zeros(3, np.uint8), 6.0)
+    assert out.shape[0] == 2 and list(mem) == [0, 0, 1]
+    np.testing.assert_allclose(out[0, 0], 1.0)
+    np.testing.assert_allclose(out[0, 1], 0.2)
+    # cov_uu = sum w (P + d^2) / W = 1 + 0.6*0.04 + 0.4*0.09
+    np.testing.assert_allclose(out[0, 7], 1 + 0.6 * 0.2 ** 2 + 0.4 * 0.3 ** 2)
+    np.testing.assert_allclose(out[1], far)
+
+
+def test_merge_flags_and_threshold(orc):
+    a = _comp([0] * 6, [1] * 6, 0.5)
+    # squared Mahalanobis with cov sum 2I: d^2/2 -> 6.0 threshold at d = sqrt(12)
+    near = _comp([np.sqrt(12) * 0.999, 0, 0, 0, 0, 0], [1] * 6, 0.1)
+    edge = _comp([np.sqrt(12) * 1.001, 0, 0, 0, 0, 0], [1] * 6, 0.1)
+    out, mem = orc.merge(np.stack([a, near, edge]), np.array([0, 0, 0], np.uint8), 6.0)
+    assert list(mem) == [0, 0, 1]
+    out, mem = orc.merge(np.stack([a, near]), np.array([0, 1], np.uint8), 6.0)
+    assert list(mem) == [0, -1] and out.shape[0] == 1
+
+
+def test_systematic_resampling_as_written(orc):
+    rng = np.random.default_rng(1)
+    for n in (1, 2, 10, 1000):
+        w = rng.exponential(size=n)
+        w /= w.sum()
+        for u in (1e-6, 0.5, 0.999999):
+            idx = orc.systematic(w, u)
+            assert np.all(np.diff(idx) >= 0)
+            r = u / n + np.arange(n) / n
+            c = np.cumsum(w)
+            want = np.minimum(np.searchsorted(c, r, side="left"), n - 1)
+            assert np.array_equal(idx, want)
+            counts = np.bincount(idx, minlength=n)
+            assert np.all(np.abs(counts - n * w) < 1 + 1e-9)
+
+
+def test_log_domain_equals_as_written_weights(pkg, orc):
+    sc = pkg.scene.make_scene(10, 3, 2.0, seed=5)
+    cfg = pkg.scene.filter_config(8, 64, 64, 2.0, precision=1, calib=sc.calib, seed=5, particles_per_feature=16)
+    a, b = orc.Oracle(cfg), orc.Oracle(cfg, weight_mode=1)
+    for k in range(sc.n_frames):
+        z = sc.frames[k]
+        for o in (a, b):
+            o.predict(0.5)
+            o.update(z[:, 0], z[:, 1], sc.fixed[k], d=z[:, 2])
+        la, lb = a.particles()[1], b.particles()[1]
+        if np.all(np.isfinite(lb)):
+            np.testing.assert_allclose(la, lb, rtol=1e-9, atol=1e-9)
+
+
+def test_fixed_camera_frames_leave_weights(pkg, orc):
+    sc = pkg.scene.make_scene(10, 2, 2.0, seed=6)
+    cfg = pkg.scene.filter_config(8, 64, 64, 2.0, precision=1, calib=sc.calib, seed=6, particles_per_feature=16)
+    o = orc.Oracle(cfg)
+    lw0 = o.particles()[1].copy()
+    o.predict(0.5)
+    z = sc.frames[0]
+    o.update(z[:, 0], z[:, 1], True, d=z[:, 2])
+    np.testing.assert_array_equal(o.particles()[1], lw0)
+
+
+def test_empty_frames_and_empty_maps(pkg, orc):
+    cfg = pkg.reference_defaults()
+    cfg.n_parents = 4
+    cfg.particles_per_feature = 8
+    o = orc.Oracle(cfg)
+    o.predict(0.5)
+    o.update(np.zeros(0), np.zeros(0), False)
+    assert np.all(o.map_sizes() == 0)
+    o.predict(0.5)
+    o.update(np.array([400.0]), np.array([300.0]), False)   # M == 1 (a reference defect case)
+    assert np.all(o.map_sizes() == 1)
+    ell, ll = o.normalizers(1)
+    np.testing.assert_allclose(ell[:, 0], np.log(1e-6 + cfg.kappa))
