@@ -1,0 +1,381 @@
+#!/usr/bin/env python
+"""Benchmark of the SC-PHD calibration filter step on B200.
+
+One step = one filter frame (predict + update + resample) of the single-filter
+workload `plain_c1` (4096 parent particles, 200 landmarks, clutter rate 50 per
+frame, <= 256 Gaussians per parent, 100 samples per Gaussian, (u,v,d)
+measurements, FP32 Kalman/merge, FP64 weights and resampling prefix).  Metric:
+Gaussian-measurement updates/s, one unit = one (parent, prior Gaussian,
+measurement) triple, counted on the device for each frame.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 runs under torchrun, one independent filter replica per GPU (weak scaling;
+the filters share nothing, so there is no data-path collective); value is the
+sum of all ranks' units over the max of the ranks' device times.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "scphd-camera-calibration_b200")
+METRIC = "Gaussian-measurement updates/s"
+UNIT = "updates/s"
+
+
+def load_package():
+    if "scphd_b200" in sys.modules:
+        return sys.modules["scphd_b200"]
+    spec = importlib.util.spec_from_file_location(
+        "scphd_b200", os.path.join(PKG_DIR, "__init__.py"), submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["scphd_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def read_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            pk = json.load(fh)
+        return float(pk["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu)], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for nm, val in zip(names, parts[5:9]):
+                    if val.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_oracle_rate(pkg, workload: str, sample_parents: int, prefill: int, frames: int, threads: int):
+    """Units/s of the FP64 oracle (the CPU restatement of the reference) on a
+    bounded sample of the workload: the same scene with `sample_parents` parents."""
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as orc
+    orc.build()
+    used = orc.set_threads(threads)
+    sc, cfg = pkg.scene.workload(workload, precision=pkg.SCPHD_FP64, n_frames=prefill + frames)
+    cfg.n_parents = sample_parents
+    o = orc.Oracle(cfg)
+    units, t = 0, 0.0
+    for k in range(prefill + frames):
+        z = sc.frames[k]
+        g = int(o.map_sizes().sum())
+        t0 = time.perf_counter()
+        o.predict(pkg.scene.DT)
+        o.update(z[:, 0], z[:, 1], sc.fixed[k], d=z[:, 2])
+        o.resample()
+        dt = time.perf_counter() - t0
+        if k >= prefill:
+            units += g * z.shape[0]
+            t += dt
+    return units / t, used, units, t
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU path (the oracle port of it) on the host cores."""
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    pkg = load_package()
+    threads = os.cpu_count() or 1
+    sample = min(4096, max(64, 2 * threads))
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as orc
+    orc.build()
+    used = orc.set_threads(threads)
+    sc, cfg = pkg.scene.workload(args.workload, precision=pkg.SCPHD_FP64,
+                                 n_frames=args.prefill + args.warmup + args.steps)
+    cfg.n_parents = sample
+    o = orc.Oracle(cfg)
+    k = 0
+    times, units = [], []
+    for phase, n in (("prefill", args.prefill), ("warmup", args.warmup), ("timed", args.steps)):
+        for _ in range(n):
+            z = sc.frames[k]
+            g = int(o.map_sizes().sum())
+            t0 = time.perf_counter()
+            o.predict(pkg.scene.DT)
+            o.update(z[:, 0], z[:, 1], sc.fixed[k], d=z[:, 2])
+            o.resample()
+            dt = time.perf_counter() - t0
+            if phase == "timed":
+                times.append(dt)
+                units.append(g * z.shape[0])
+            k += 1
+    value = sum(units) / sum(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "n_parents": sample, "n_parents_full": 4096,
+                   "note": "parent sample of the workload; units/s is per-parent-additive"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": "port",
+                         "sample": f"{sample} of 4096 parents of {args.workload}, {args.prefill} untimed frames "
+                                   f"to populate the maps, then {args.warmup}+{args.steps} frames"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args):
+    import torch
+    world, rank, local = dist_env()
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    pkg = load_package()
+    prec = pkg.SCPHD_FP32 if args.precision == "fp32" else pkg.SCPHD_FP64
+    K, W = args.steps, args.warmup
+    n_frames = args.prefill + W + 3 * K + 1
+    sc, cfg = pkg.scene.workload(args.workload, precision=prec, filter_index=rank, n_frames=n_frames)
+    if args.parents:
+        cfg.n_parents = args.parents   # smaller case for profiler captures; not a bench line
+    cfg.device = local
+    filt = pkg.SCPHDCameraCalibration(cfg)
+    dev = torch.device("cuda", local)
+    dframes = []
+    for z in sc.frames:
+        zt = torch.tensor(np.ascontiguousarray(z.T), dtype=torch.float64, device=dev).contiguous()
+        dframes.append(zt)
+    torch.cuda.synchronize()
+    k = 0
+
+    def dstep():
+        nonlocal k
+        zt = dframes[k]
+        filt.step_device(pkg.scene.DT, zt[0].data_ptr(), zt[1].data_ptr(), zt[2].data_ptr(), zt.shape[1],
+                         sc.fixed[k])
+        k += 1
+
+    for _ in range(args.prefill + W):
+        dstep()
+    filt.synchronize()
+    stream = torch.cuda.ExternalStream(filt.stream_handle)
+    c0 = filt.counters()
+    l0 = pkg.kernel_launches()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(K + 1)]
+    ev[0].record(stream)
+    for i in range(K):
+        dstep()
+        ev[i + 1].record(stream)
+    ev[K].synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms_total = ev[0].elapsed_time(ev[K])
+    frame_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(K)]
+    c1 = filt.counters()
+    launches = pkg.kernel_launches() - l0
+    units = int(c1[6] - c0[6])
+    # per-stage device times (events around each stage on the filter's stream)
+    filt.set_profiling(True)
+    c_p0 = filt.counters()
+    for _ in range(K):
+        dstep()
+    stages = filt.stage_times()
+    filt.set_profiling(False)
+    c_p1 = filt.counters()
+    # end to end through the host-array C ABI: H2D of the frame, step, D2H of the result
+    h2d = d2h = 0
+    ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ce0 = filt.counters()
+    torch.cuda.synchronize()
+    ee0.record(stream)
+    for _ in range(K):
+        z = sc.frames[k]
+        filt.step(pkg.scene.DT, z[:, 0], z[:, 1], sc.fixed[k], d=z[:, 2])
+        st, lw = filt.particles()
+        h2d += 3 * 8 * z.shape[0]
+        d2h += st.nbytes + lw.nbytes
+        k += 1
+    ee1.record(stream)
+    ee1.synchronize()
+    ce1 = filt.counters()
+    e2e_ms = ee0.elapsed_time(ee1)
+    e2e_units = int(ce1[6] - ce0[6])
+
+    tot = torch.tensor([ms_total, float(units), e2e_ms, float(e2e_units)], dtype=torch.float64, device=dev)
+    if dist:
+        mx = tot.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = tot.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        ms_all, units_all, e2e_ms_all, e2e_units_all = mx[0].item(), sm[1].item(), mx[2].item(), sm[3].item()
+    else:
+        ms_all, units_all, e2e_ms_all, e2e_units_all = ms_total, float(units), e2e_ms, float(e2e_units)
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    value = units_all / (ms_all / 1e3)
+    e2e_value = e2e_units_all / (e2e_ms_all / 1e3)
+
+    # roofline of the dominant stage
+    peak, peak_kind = read_peaks()
+    sz = 4 if prec == pkg.SCPHD_FP32 else 8
+    P = int(cfg.particles_per_feature)
+    dom = max(stages.items(), key=lambda kv: kv[1][0])
+    name, (stage_ms, n_launch) = dom
+    fitted = c_p1[10] - c_p0[10]
+    rd, wr = c_p1[8] - c_p0[8], c_p1[9] - c_p0[9]
+    surv = c_p1[7] - c_p0[7]
+    merged = c_p1[11] - c_p0[11]
+    algo_bytes = {
+        # map entry read (28) + fitted row (29) + Kalman terms (47) per Gaussian, clouds read/written
+        "cloud_fit": fitted * (28 + 29 + 47) * sz + (rd + wr) * 7 * P * sz,
+        # Kalman terms + fitted mean read per (parent, Gaussian), survivors written
+        "likelihood": fitted * (8 + 3) * sz * 2 + surv * (4 + sz),
+        # survivors read, merged rows written, new map rows written
+        "merge": surv * (4 + sz) + merged * 28 * sz * 2,
+    }.get(name, 0)
+    per_launch = algo_bytes / max(1, n_launch)
+    avg_ms = stage_ms / max(1, n_launch)
+    achieved = per_launch / (avg_ms / 1e3) / 1e9 if avg_ms > 0 else 0.0
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as fh:
+            tr = json.load(fh).get(name)
+        if tr:
+            traffic = tr.get("bytes_per_launch_scaled")
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        sample = min(4096, max(32, threads))
+        rate, used, cu, ct = cpu_oracle_rate(pkg, args.workload, sample, args.cpu_prefill, args.cpu_frames, threads)
+        cpu = {"value": rate, "unit": UNIT, "cores": used, "kind": "port",
+               "sample": f"{sample} of {cfg.n_parents} parents of {args.workload}, {args.cpu_prefill} untimed "
+                         f"frames to populate the maps, {args.cpu_frames} timed frames ({ct:.1f} s)"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms_all / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": args.precision, "data": "synthetic",
+        "config": {"workload": args.workload, "n_parents": int(cfg.n_parents), "landmarks": 200,
+                   "clutter_rate": 50.0, "max_gaussians": int(cfg.max_gaussians),
+                   "particles_per_feature": P, "meas_dim": int(cfg.meas_dim), "prefill_frames": args.prefill,
+                   "mean_gaussians_per_parent": fitted / max(1, K) / cfg.n_parents,
+                   "mean_measurements": units / max(1, fitted / K * 1.0) / K if fitted else None,
+                   "l2": "no flush: the resident map/cloud state is larger than L2",
+                   "parallelism": f"replicas{world}"},
+        "frame_ms": {"p50": float(np.percentile(frame_ms, 50)), "p99": float(np.percentile(frame_ms, 99)),
+                     "max": float(max(frame_ms))},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d // K, "d2h_bytes_per_step": d2h // K},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": avg_ms},
+        "stage_ms_per_frame": {k2: v[0] / max(1, v[1]) for k2, v in stages.items()},
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "counters": {"truncations": int(c1[0]), "scratch_overflows": int(c1[1])},
+    }
+    print(json.dumps(line), flush=True)
+    filt.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="plain_c1")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--prefill", type=int, default=30)
+    ap.add_argument("--cpu-prefill", type=int, default=30)
+    ap.add_argument("--cpu-frames", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--parents", type=int, default=0, help="override the parent count (profiling only)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -111,6 +111,10 @@ scphd_status scphd_resample(scphd_filter* f, int32_t* resampled);
 scphd_status scphd_step(scphd_filter* f, double dt, const double* u, const double* v,
                         const double* d, int32_t n, int32_t fixed_camera);
 
+/* scphd_step with DEVICE measurement arrays (FP64; d may be NULL in (u,v) mode). */
+scphd_status scphd_step_device(scphd_filter* f, double dt, const double* u_dev, const double* v_dev,
+                               const double* d_dev, int32_t n, int32_t fixed_camera);
+
 /* checkStuff(): SCPHD_ERR_NAN if any parent weight is NaN. */
 scphd_status scphd_check(scphd_filter* f);
 
@@ -161,8 +165,23 @@ scphd_status scphd_set_state(scphd_filter* f, const double* states, const double
 /* Counters since create: [0] map truncations at max_gaussians, [1] merge-scratch
  * overflows at max_survivors, [2] frames updated, [3] resamplings,
  * [4] Gaussian-measurement units of the last update (sum_p G_p * n),
- * [5] survivors of the last update (sum over parents). */
-scphd_status scphd_get_counters(scphd_filter* f, int64_t counters[8]);
+ * [5] survivors of the last update (sum over parents), [6] units since create,
+ * [7] survivors since create, [8] sample clouds read from memory, [9] sample
+ * clouds written, [10] Gaussians fitted, [11] merged components produced,
+ * [12] full Mahalanobis evaluations in the merge; [13..15] reserved. */
+scphd_status scphd_get_counters(scphd_filter* f, int64_t counters[16]);
+
+/* The CUDA stream (a cudaStream_t) all of the handle's work is issued on, so a
+ * caller can order its own work or timing events after the filter's. */
+void* scphd_stream(scphd_filter* f);
+
+/* Per-stage device timing with CUDA events recorded on the handle's stream around
+ * each stage's kernel (off by default).  Stages: 0 parent prediction, 1 cloud
+ * fit, 2 likelihood/survivors, 3 merge, 4 parent weights, 5 resampling.
+ * scphd_get_stage_times synchronises the stream, returns the summed milliseconds
+ * and launch counts per stage since the last call, and clears them. */
+scphd_status scphd_set_profiling(scphd_filter* f, int32_t enable);
+scphd_status scphd_get_stage_times(scphd_filter* f, double ms[8], int64_t launches[8]);
 
 /* Stand-alone stages on caller-provided HOST data, for parity checks of the
  * device code paths the step uses.

@@ -67,7 +67,50 @@ struct scphd_filter {
     uint32_t pending_frame = 0;
     uint32_t sample_frame[2] = {0, 0};
     int last_M = 0;
-    virtual ~scphd_filter() {}
+    // opt-in per-stage event timing
+    bool profiling = false;
+    struct Mark { int stage; cudaEvent_t a, b; };
+    std::vector<Mark> marks;
+    std::vector<cudaEvent_t> event_pool;
+    size_t pool_next = 0;
+    double stage_ms[8] = {0};
+    long long stage_n[8] = {0};
+    cudaEvent_t take_event() {
+        if (pool_next >= event_pool.size()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            event_pool.push_back(e);
+        }
+        return event_pool[pool_next++];
+    }
+    // begin/end of one stage's launch on the stream (no-ops unless profiling)
+    int stage_begin(int stage) {
+        if (!profiling) return -1;
+        if (marks.size() > 8192) flush_marks();
+        Mark m{stage, take_event(), take_event()};
+        cudaEventRecord(m.a, stream);
+        marks.push_back(m);
+        return (int)marks.size() - 1;
+    }
+    void stage_end(int h) {
+        if (h < 0) return;
+        cudaEventRecord(marks[h].b, stream);
+    }
+    void flush_marks() {
+        cudaStreamSynchronize(stream);
+        for (const Mark& m : marks) {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, m.a, m.b) == cudaSuccess) {
+                stage_ms[m.stage] += ms;
+                stage_n[m.stage] += 1;
+            }
+        }
+        marks.clear();
+        pool_next = 0;
+    }
+    virtual ~scphd_filter() {
+        for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
+    }
     virtual scphd_status init() = 0;
     virtual scphd_status predict(double dt) = 0;
     virtual scphd_status update_staged(int M, int fixed) = 0;
@@ -150,13 +193,14 @@ public:
         b.surv_w = a.take<T>(N * S);
         b.surv_n = a.take<int>(N);
         b.merged = a.take<T>(N * S * kRow);
+        b.mtmp = a.take<T>(N * S * kRow);
         b.merged_n = a.take<int>(N);
         b.loglik = a.take<double>(N);
         b.cum = a.take<double>(N);
         b.scal = a.take<double>(4);
         b.flags = a.take<int>(4);
         b.resample_idx = a.take<int>(N);
-        b.counters = a.take<unsigned long long>(8);
+        b.counters = a.take<unsigned long long>(16);
         dump = a.take<T>(G * 7 * Ps);
         fit_n = a.take<int>(N);
         d_stage = a.take<double>(Mc * 3);
@@ -179,7 +223,11 @@ public:
         a.cap = probe.used;
         carve(a);
         CUDA_TRY(cudaMemsetAsync(p, 0, probe.used, stream));
-        merge_smem = (size_t)2 * prm.Scap * (sizeof(T) + 8) + (size_t)6 * prm.Scap * sizeof(T) + prm.Scap + 64;
+        {
+            const size_t S = prm.Scap, G = prm.Gcap, S2 = 2 * S + 2 * G, nchunk = (S + 31) / 32;
+            merge_smem = S2 * (sizeof(T) + 8) + 6 * S * sizeof(T) + 2 * S * 4 + (S + G) * 4 + 4 * nchunk * 4 +
+                         2 * S + 64;
+        }
         if (prm.K == 2) {
             CUDA_TRY(cudaFuncSetAttribute(k_merge<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem));
         } else {
@@ -214,8 +262,10 @@ public:
         frame++;
         if (frame >= (1u << 20)) return fail(SCPHD_ERR_CAPACITY, "frame counter exhausted (2^20 frames)");
         const int N = prm.N;
+        int h = stage_begin(0);
         k_predict_parents<<<(N + 255) / 256, 256, 0, stream>>>(prm, b.ext, dt, frame);
         LAUNCHED();
+        stage_end(h);
         pending = true;
         pending_dt = dt;
         pending_frame = frame;
@@ -225,6 +275,7 @@ public:
     template <int K> scphd_status update_k(int M, int fixed) {
         const int N = prm.N;
         CUDA_TRY(cudaMemsetAsync(b.counters + 4, 0, 2 * sizeof(unsigned long long), stream));
+        int h = stage_begin(1);
         if (prm.P <= 128)
             k_cloud_fit<T, K, 4><<<N, 256, 0, stream>>>(prm, b, cur, M, fixed, pending ? 1 : 0, pending_dt,
                                                          pending_frame, sample_frame[cur]);
@@ -232,16 +283,23 @@ public:
             k_cloud_fit<T, K, 8><<<N, 256, 0, stream>>>(prm, b, cur, M, fixed, pending ? 1 : 0, pending_dt,
                                                          pending_frame, sample_frame[cur]);
         LAUNCHED();
+        stage_end(h);
         pending = false;
         if (M > 0) {
             dim3 grid(N, (M + 127) / 128);
+            h = stage_begin(2);
             k_likelihood<T, K><<<grid, 128, 0, stream>>>(prm, b, cur, M);
             LAUNCHED();
+            stage_end(h);
         }
+        h = stage_begin(3);
         k_merge<T, K><<<N, 128, merge_smem, stream>>>(prm, b, cur, M, fixed);
         LAUNCHED();
+        stage_end(h);
+        h = stage_begin(4);
         k_weights<<<1, 1024, 0, stream>>>(N, b.lw, b.loglik, fixed ? 0 : 1, b.scal);
         LAUNCHED();
+        stage_end(h);
         return SCPHD_OK;
     }
 
@@ -272,9 +330,11 @@ public:
     }
 
     scphd_status resample(int32_t* resampled, bool read_back) override {
+        int h = stage_begin(5);
         k_resample<<<1, 1024, 0, stream>>>(prm, b.lw, b.ext, b.ext_tmp, b.src, b.src_tmp, b.cum, b.scal, b.flags,
                                            b.resample_idx, frame, 0, -1.0, b.counters);
         LAUNCHED();
+        stage_end(h);
         if (read_back) {
             int f = 0;
             CUDA_TRY(cudaMemcpyAsync(&f, b.flags, sizeof(int), cudaMemcpyDeviceToHost, stream));
@@ -426,10 +486,10 @@ public:
     }
 
     scphd_status get_counters(int64_t* c) override {
-        unsigned long long h[8];
+        unsigned long long h[16];
         CUDA_TRY(cudaMemcpyAsync(h, b.counters, sizeof(h), cudaMemcpyDeviceToHost, stream));
         CUDA_TRY(cudaStreamSynchronize(stream));
-        for (int i = 0; i < 8; ++i) c[i] = (int64_t)h[i];
+        for (int i = 0; i < 16; ++i) c[i] = (int64_t)h[i];
         return SCPHD_OK;
     }
 
@@ -614,6 +674,25 @@ scphd_status scphd_step(scphd_filter* f, double dt, const double* u, const doubl
     return f->resample(nullptr, false);
 }
 
+scphd_status scphd_step_device(scphd_filter* f, double dt, const double* u, const double* v, const double* d,
+                               int32_t n, int32_t fixed_camera) {
+    HANDLE(f);
+    if (!std::isfinite(dt)) return fail(SCPHD_ERR_INVALID, "dt must be finite");
+    if (n < 0) return fail(SCPHD_ERR_INVALID, "negative measurement count");
+    if (n > f->prm.Mcap) return fail(SCPHD_ERR_CAPACITY, "more measurements than max_measurements");
+    if (f->prm.K == 3 && n > 0 && !d) return fail(SCPHD_ERR_INVALID, "meas_dim 3 needs the disparity array");
+    if (n > 0) {
+        CUDA_TRY(cudaMemcpyAsync(f->d_stage, u, sizeof(double) * n, cudaMemcpyDeviceToDevice, f->stream));
+        CUDA_TRY(cudaMemcpyAsync(f->d_stage + n, v, sizeof(double) * n, cudaMemcpyDeviceToDevice, f->stream));
+        if (d) CUDA_TRY(cudaMemcpyAsync(f->d_stage + 2 * n, d, sizeof(double) * n, cudaMemcpyDeviceToDevice, f->stream));
+    }
+    scphd_status s = f->predict(dt);
+    if (s != SCPHD_OK) return s;
+    s = f->update_staged(n, fixed_camera ? 1 : 0);
+    if (s != SCPHD_OK) return s;
+    return f->resample(nullptr, false);
+}
+
 scphd_status scphd_check(scphd_filter* f) {
     HANDLE(f);
     return f->check();
@@ -672,7 +751,7 @@ scphd_status scphd_set_state(scphd_filter* f, const double* states, const double
     return f->set_state(states, log_weights, sizes, weights, clouds, omega);
 }
 
-scphd_status scphd_get_counters(scphd_filter* f, int64_t counters[8]) {
+scphd_status scphd_get_counters(scphd_filter* f, int64_t counters[16]) {
     HANDLE(f);
     if (!counters) return fail(SCPHD_ERR_INVALID, "null output");
     return f->get_counters(counters);
@@ -696,7 +775,9 @@ scphd_status scphd_merge_components(const double* comps, const uint8_t* flags, i
         uint8_t* d_flags = nullptr;
         int* d_n = nullptr;
         int* d_mem = nullptr;
-        size_t smem = (size_t)(2 * n + 2) * (sizeof(T) + 8) + (size_t)(6 * n + 6) * sizeof(T) + n + 64;
+        const size_t cap = (size_t)n + 1, nchunk = (cap + 31) / 32;
+        size_t smem = 2 * cap * (sizeof(T) + 8) + 6 * cap * sizeof(T) + 3 * cap * 4 + 4 * nchunk * 4 + 2 * cap + 64;
+        T* d_sparse = nullptr;
         scphd_status st = SCPHD_OK;
         std::vector<T> out((size_t)n * kRow);
         int nout = 0;
@@ -705,7 +786,8 @@ scphd_status scphd_merge_components(const double* comps, const uint8_t* flags, i
             if (cudaMalloc(&d_rows, sizeof(T) * rows.size()) != cudaSuccess ||
                 cudaMalloc(&d_out, sizeof(T) * rows.size()) != cudaSuccess ||
                 cudaMalloc(&d_flags, n) != cudaSuccess || cudaMalloc(&d_n, sizeof(int)) != cudaSuccess ||
-                cudaMalloc(&d_mem, sizeof(int) * n) != cudaSuccess) {
+                cudaMalloc(&d_mem, sizeof(int) * n) != cudaSuccess ||
+                cudaMalloc(&d_sparse, sizeof(T) * rows.size()) != cudaSuccess) {
                 st = fail(SCPHD_ERR_CUDA, "allocation for merge_components failed");
                 break;
             }
@@ -713,7 +795,7 @@ scphd_status scphd_merge_components(const double* comps, const uint8_t* flags, i
             cudaMemcpy(d_flags, flags, n, cudaMemcpyHostToDevice);
             cudaMemset(d_mem, 0xff, sizeof(int) * n);
             cudaFuncSetAttribute(k_merge_list<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            k_merge_list<T><<<1, 128, smem>>>(d_rows, d_flags, n, (T)min_separation, d_out, d_n, d_mem);
+            k_merge_list<T><<<1, 128, smem>>>(d_rows, d_flags, n, (T)min_separation, d_sparse, d_out, d_n, d_mem);
             g_launches.fetch_add(1, std::memory_order_relaxed);
             cudaError_t e = cudaDeviceSynchronize();
             if (e != cudaSuccess) {
@@ -724,7 +806,7 @@ scphd_status scphd_merge_components(const double* comps, const uint8_t* flags, i
             cudaMemcpy(out.data(), d_out, sizeof(T) * out.size(), cudaMemcpyDeviceToHost);
             cudaMemcpy(mem.data(), d_mem, sizeof(int) * n, cudaMemcpyDeviceToHost);
         } while (0);
-        cudaFree(d_rows); cudaFree(d_out); cudaFree(d_flags); cudaFree(d_n); cudaFree(d_mem);
+        cudaFree(d_rows); cudaFree(d_out); cudaFree(d_flags); cudaFree(d_n); cudaFree(d_mem); cudaFree(d_sparse);
         if (st != SCPHD_OK) return st;
         *n_out = nout;
         for (int i = 0; i < nout; ++i)
@@ -770,6 +852,27 @@ scphd_status scphd_systematic_resample(const double* weights, int32_t n, double 
     cudaFree(d_lw); cudaFree(d_ext); cudaFree(d_ext_tmp); cudaFree(d_cum); cudaFree(d_scal);
     cudaFree(d_src); cudaFree(d_src_tmp); cudaFree(d_flags); cudaFree(d_idx);
     return st;
+}
+
+void* scphd_stream(scphd_filter* f) { return f ? (void*)f->stream : nullptr; }
+
+scphd_status scphd_set_profiling(scphd_filter* f, int32_t enable) {
+    HANDLE(f);
+    if (!enable && f->profiling) f->flush_marks();
+    f->profiling = enable != 0;
+    return SCPHD_OK;
+}
+
+scphd_status scphd_get_stage_times(scphd_filter* f, double ms[8], int64_t launches[8]) {
+    HANDLE(f);
+    f->flush_marks();
+    for (int i = 0; i < 8; ++i) {
+        if (ms) ms[i] = f->stage_ms[i];
+        if (launches) launches[i] = f->stage_n[i];
+        f->stage_ms[i] = 0;
+        f->stage_n[i] = 0;
+    }
+    return SCPHD_OK;
 }
 
 const char* scphd_last_error(void) { return g_err.c_str(); }

@@ -51,13 +51,14 @@ template <typename T> struct Bufs {
     T* surv_w;          // N x Scap survivor weights
     int* surv_n;        // N
     T* merged;          // N x Scap rows of kRow (merge output, in order)
+    T* mtmp;            // N x Scap rows of kRow (merge output indexed by centre)
     int* merged_n;      // N
     double* loglik;     // N
     double* cum;        // N resampling prefix
     double* scal;       // [0] neff
     int* flags;         // [0] resampled
     int* resample_idx;  // N
-    unsigned long long* counters;   // 8
+    unsigned long long* counters;   // 16
 };
 
 __device__ __forceinline__ uint32_t tie_key(uint32_t r) {
@@ -130,17 +131,22 @@ __global__ void __launch_bounds__(256) k_cloud_fit(Params prm, Bufs<T> b, int cu
         pose_src = make_pose<T>(b.map_ext[cur] + 12 * row);
         b.surv_n[p] = 0;
         atomicAdd(&b.counters[4], (unsigned long long)G * (unsigned long long)M);
+        atomicAdd(&b.counters[6], (unsigned long long)G * (unsigned long long)M);
     }
     __syncthreads();
     const Model& m = prm.model;
     const int P = prm.P, Ps = prm.Ps;
     const T invP = T(1) / T(P);
+    __shared__ int s_rd, s_wr;
+    if (threadIdx.x == 0) { s_rd = 0; s_wr = 0; }
+    __syncthreads();
     for (int j = warp; j < G; j += blockDim.x >> 5) {
         const size_t erow = (size_t)row * prm.Gcap + j;
         const T* ent = b.map[cur] + erow * kRow;
         const int ref = b.map_ref[cur][erow];
         T W = ent[0];
         T X[NS][6], om[NS];
+        if (lane == 0 && ref >= 0) atomicAdd(&s_rd, 1);
         if (ref < 0) {   // merged component: regenerate its sample cloud (.cu:640-690 + :1222-1286)
             T L[21];
             chol6(ent + 7, L);
@@ -287,6 +293,7 @@ __global__ void __launch_bounds__(256) k_cloud_fit(Params prm, Bufs<T> b, int cu
         // retained non-detection cloud: predicted world samples, weights 1 - pD
         const T wnd = W * (T(1) - pbar);
         if (wnd >= (T)prm.min_weight) {
+            if (lane == 0) atomicAdd(&s_wr, 1);
             T* cl = b.cloud[cur ^ 1] + ((size_t)p * prm.Gcap + j) * 7 * Ps;
 #pragma unroll
             for (int t = 0; t < NS; ++t) {
@@ -298,6 +305,12 @@ __global__ void __launch_bounds__(256) k_cloud_fit(Params prm, Bufs<T> b, int cu
                 }
             }
         }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        atomicAdd(&b.counters[8], (unsigned long long)s_rd);
+        atomicAdd(&b.counters[9], (unsigned long long)s_wr);
+        atomicAdd(&b.counters[10], (unsigned long long)G);
     }
 }
 
@@ -496,109 +509,209 @@ __device__ void sort_survivors(T* s_w, uint32_t* s_key, int* s_r, int n_pad) {
     }
 }
 
-// Greedy reduction of phdUpdateMergeKernel (src/kernels.cu:693-866) over n sorted
-// survivors: the next centre is the first unmerged one in sorted order (the
-// reference's argmax sequence), every unmerged survivor within squared
-// Mahalanobis distance < min_sep of the centre (covariance sum) is absorbed, the
-// moment-matched result is kept if PD, else the centre.  A diagonal bound
-// (x' A^-1 x >= x_k^2 / A_kk for SPD A) skips the full distance for pairs that
-// cannot merge; pairs within a safety margin of the bound are evaluated fully.
-// Outputs rows of kRow to out[0..), returns the count.  Block-wide call.
+// Block-wide exclusive scan of int flags (n <= blockDim * 64); returns the total.
+__device__ int block_exclusive_scan(int* data, int n, int* s_tmp) {
+    const int per = (n + blockDim.x - 1) / blockDim.x;
+    const int lo = threadIdx.x * per, hi = min(n, lo + per);
+    int run = 0;
+    for (int i = lo; i < hi; ++i) { int v = data[i]; data[i] = run; run += v; }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int v = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    if (lane == 31) s_tmp[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int w = 0; w < nw; ++w) { int t = s_tmp[w]; s_tmp[w] = acc; acc += t; }
+        s_tmp[nw] = acc;
+    }
+    __syncthreads();
+    const int off = s_tmp[warp] + v - run;
+    for (int i = lo; i < hi; ++i) data[i] += off;
+    const int total = s_tmp[nw];
+    __syncthreads();
+    return total;
+}
+
+// lock-free union-find on shared memory: roots only change by CAS from a self
+// loop, the larger root is attached under the smaller, so every component's root
+// is its smallest index
+__device__ __forceinline__ int uf_find(int* uf, int x) {
+    int p = uf[x];
+    while (p != x) {
+        int gp = uf[p];
+        if (gp != p) uf[x] = gp;   // path halving; only ever points closer to the root
+        x = p;
+        p = uf[x];
+    }
+    return x;
+}
+__device__ __forceinline__ void uf_unite(int* uf, int a, int b) {
+    while (true) {
+        a = uf_find(uf, a);
+        b = uf_find(uf, b);
+        if (a == b) return;
+        if (a < b) { int t = a; a = b; b = t; }
+        if (atomicCAS(&uf[a], a, b) == a) return;
+    }
+}
+
+template <typename T> struct MergeScratch {
+    T* pf;          // n x 6: mean[0..3), cov diagonal [0..3) (prefilter data)
+    uint8_t* flag;  // n: merged
+    uint8_t* is_center;   // n
+    int* uf;        // n: union-find parent, then component label (= smallest index)
+    int* roots;     // n
+    uint32_t* masks;      // (blockDim/32) x nchunk member masks
+    int nchunk;
+};
+
+template <typename T>
+__device__ __forceinline__ bool could_merge(const T* a, const T* b, T min_sep, T margin) {
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        T d = a[k] - b[k];
+        ok = ok && (d * d <= min_sep * (a[3 + k] + b[3 + k]) * margin);
+    }
+    return ok;
+}
+
+// Greedy reduction of phdUpdateMergeKernel (src/kernels.cu:693-866) over n
+// survivors already sorted into the reference's argmax order: the next centre is
+// the first unmerged survivor, every unmerged survivor within squared Mahalanobis
+// distance < min_sep of it (covariance sum) is absorbed, the moment-matched result
+// is kept if PD, else the centre.  Since x' A^-1 x >= x_k^2 / A_kk for SPD A, two
+// survivors failing the diagonal bound on u, v or d (with a safety margin) can
+// never merge; the greedy sequence therefore decomposes exactly over the connected
+// components of the "may merge" graph, and each warp runs the greedy loop on whole
+// components independently.  Merged rows are written to sparse[centre index];
+// returns the index of the first centre that absorbed nothing (the reference's
+// loop ends there), or n.  Block-wide call.
 template <typename T, typename Src>
-__device__ int merge_loop(const Src& src, const T* s_w, const int* s_r, int n, T* s_pf, uint8_t* s_flag,
-                          T min_sep, T margin, T* out, int out_cap, int* member_out) {
-    __shared__ int s_center, s_nmem;
-    __shared__ T s_cmu[6], s_ccov[21];
-    __shared__ T s_acc[28];
-    const int tid = threadIdx.x;
-    const int warp = tid >> 5, lane = tid & 31;
-    // prefilter data: mean[0..3) and cov diagonal [0..3) per survivor
+__device__ int merge_components(const Src& src, const T* s_w, const int* s_r, int n, MergeScratch<T> ms,
+                                T min_sep, T margin, T* sparse, int* member_out, unsigned long long* counters) {
+    __shared__ int s_nroots, s_take, s_stop, s_evals, s_ncent;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int i = tid; i < n; i += blockDim.x) {
         T mu[6];
         src.mean(s_r[i], mu);
         const T* cv = src.cov(s_r[i]);
-        s_pf[i * 6 + 0] = mu[0]; s_pf[i * 6 + 1] = mu[1]; s_pf[i * 6 + 2] = mu[2];
-        s_pf[i * 6 + 3] = cv[0]; s_pf[i * 6 + 4] = cv[2]; s_pf[i * 6 + 5] = cv[5];
-        s_flag[i] = 0;
+        ms.pf[i * 6 + 0] = mu[0]; ms.pf[i * 6 + 1] = mu[1]; ms.pf[i * 6 + 2] = mu[2];
+        ms.pf[i * 6 + 3] = cv[0]; ms.pf[i * 6 + 4] = cv[2]; ms.pf[i * 6 + 5] = cv[5];
+        ms.flag[i] = 0;
+        ms.is_center[i] = 0;
+        ms.uf[i] = i;
+    }
+    if (tid == 0) { s_nroots = 0; s_take = 0; s_stop = n; s_evals = 0; s_ncent = 0; }
+    __syncthreads();
+    // "may merge" edges -> components
+    for (int i = tid; i < n; i += blockDim.x) {
+        const T* a = ms.pf + i * 6;
+        for (int j = i + 1; j < n; ++j)
+            if (could_merge(a, ms.pf + j * 6, min_sep, margin)) uf_unite(ms.uf, i, j);
     }
     __syncthreads();
-    int next = 0, n_out = 0;
+    for (int i = tid; i < n; i += blockDim.x) {
+        int r = uf_find(ms.uf, i);
+        if (r == i) ms.roots[atomicAdd(&s_nroots, 1)] = i;
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += blockDim.x) ms.uf[i] = uf_find(ms.uf, i);
+    __syncthreads();
+    uint32_t* masks = ms.masks + (size_t)warp * ms.nchunk;
+    const int nch = (n + 31) >> 5;   // <= ms.nchunk
+    int evals = 0;
     while (true) {
-        if (tid == 0) {
-            while (next < n && s_flag[next]) ++next;
-            s_center = next < n ? next : -1;
-            s_nmem = 0;
-            if (next < n) {
-                T mu[6];
-                src.mean(s_r[next], mu);
-                const T* cv = src.cov(s_r[next]);
-                for (int a = 0; a < 6; ++a) s_cmu[a] = mu[a];
-                for (int i = 0; i < 21; ++i) s_ccov[i] = cv[i];
-            }
-        }
-        __syncthreads();
-        const int c = s_center;
-        if (c < 0) break;
-        // mark members (flag 2)
-        for (int i = tid; i < n; i += blockDim.x) {
-            if (s_flag[i]) continue;
-            bool cand = true;
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                T d = s_cmu[k] - s_pf[i * 6 + k];
-                T a = s_ccov[tri(k, k)] + s_pf[i * 6 + 3 + k];
-                cand = cand && (d * d <= min_sep * a * margin);
-            }
-            if (!cand) continue;
-            T mu[6];
-            src.mean(s_r[i], mu);
-            T dist = mahal6(s_cmu, s_ccov, mu, src.cov(s_r[i]));
-            if (dist < min_sep) {
-                s_flag[i] = 2;
-                atomicAdd(&s_nmem, 1);
-            }
-        }
-        __syncthreads();
-        // no member (not even the centre itself, e.g. a NaN distance): the reference's
-        // merged weight is 0 and its loop ends (kernels.cu:783-784)
-        if (s_nmem == 0) break;
-        if (warp == 0) {
-            // pass 1: weight and mean, members in index order
-            T accw = 0, accm = 0;   // lane a < 6 accumulates mean[a]
-            for (int base = 0; base < n; base += 32) {
+        int comp = 0;
+        if (lane == 0) comp = atomicAdd(&s_take, 1);
+        comp = __shfl_sync(0xffffffffu, comp, 0);
+        if (comp >= s_nroots) break;
+        const int r = ms.roots[comp];
+        int next = r;
+        while (true) {
+            // centre: first unmerged member of the component
+            int c = -1;
+            for (int base = next & ~31; base < n; base += 32) {
                 int i = base + lane;
-                unsigned mask = __ballot_sync(0xffffffffu, i < n && s_flag[i] == 2);
-                while (mask) {
-                    int l = __ffs(mask) - 1;
-                    mask &= mask - 1;
-                    int ii = base + l;
+                bool pred = i >= next && i < n && ms.uf[i] == r && !ms.flag[i];
+                unsigned bal = __ballot_sync(0xffffffffu, pred);
+                if (bal) { c = base + __ffs(bal) - 1; break; }
+            }
+            if (c < 0) break;
+            next = c + 1;
+            T cmu[6], ccov[21];
+            src.mean(s_r[c], cmu);
+            const T* cc = src.cov(s_r[c]);
+#pragma unroll
+            for (int q = 0; q < 21; ++q) ccov[q] = cc[q];
+            // members: unmerged survivors of the component within distance
+            const int c0 = c >> 5;
+            bool any = false;
+            for (int ch = c0; ch < nch; ++ch) {
+                int i = ch * 32 + lane;
+                bool mem = false;
+                if (i >= c && i < n && ms.uf[i] == r && !ms.flag[i]) {
+                    T pfc[6] = {cmu[0], cmu[1], cmu[2], ccov[0], ccov[2], ccov[5]};
+                    if (could_merge(pfc, ms.pf + i * 6, min_sep, margin)) {
+                        ++evals;
+                        T mu[6];
+                        src.mean(s_r[i], mu);
+                        mem = mahal6(cmu, ccov, mu, src.cov(s_r[i])) < min_sep;
+                    }
+                }
+                unsigned bal = __ballot_sync(0xffffffffu, mem);
+                if (lane == 0) masks[ch] = bal;
+                any = any || bal;
+            }
+            __syncwarp();
+            if (!any) {   // merged weight 0: the reference's loop ends (kernels.cu:783-784)
+                if (lane == 0) atomicMin(&s_stop, c);
+                break;
+            }
+            // weight and mean, members in index order; lane a < 6 owns mean[a]
+            T accw = 0, accm = 0;
+            for (int ch = c0; ch < nch; ++ch) {
+                unsigned mk = masks[ch];
+                while (mk) {
+                    int ii = ch * 32 + __ffs(mk) - 1;
+                    mk &= mk - 1;
                     T w = s_w[ii];
                     T mu[6];
                     src.mean(s_r[ii], mu);
                     accw += w;
-                    if (lane < 6) accm += w * mu[lane];
+                    T sel = mu[0];
+#pragma unroll
+                    for (int a = 1; a < 6; ++a) sel = (lane == a) ? mu[a] : sel;
+                    if (lane < 6) accm += w * sel;
                 }
             }
-            T W = accw;
-            T mean_l = (lane < 6) ? accm / W : T(0);
-            if (lane < 6) s_acc[1 + lane] = mean_l;
-            __syncwarp();
+            const T W = accw;
             T mean[6];
+            const T my_mean = (lane < 6) ? accm / W : T(0);
 #pragma unroll
-            for (int a = 0; a < 6; ++a) mean[a] = s_acc[1 + a];
-            // pass 2: covariance (lane e < 21 owns packed entry e)
-            int ea = 0, eb = 0;
-            if (lane < 21) { ea = 0; while ((ea + 1) * (ea + 2) / 2 <= lane) ++ea; eb = lane - ea * (ea + 1) / 2; }
+            for (int a = 0; a < 6; ++a) mean[a] = __shfl_sync(0xffffffffu, my_mean, a);
+            // covariance: lane e < 21 owns packed entry e = (ea, eb)
+            int ea = 0;
+            while ((ea + 1) * (ea + 2) / 2 <= lane && ea < 5) ++ea;
+            const int eb = lane - ea * (ea + 1) / 2;
             T accc = 0;
-            for (int base = 0; base < n; base += 32) {
-                int i = base + lane;
-                unsigned mask = __ballot_sync(0xffffffffu, i < n && s_flag[i] == 2);
-                while (mask) {
-                    int l = __ffs(mask) - 1;
-                    mask &= mask - 1;
-                    int ii = base + l;
-                    T w = s_w[ii];
+            for (int ch = c0; ch < nch; ++ch) {
+                unsigned mk = masks[ch];
+                int i = ch * 32 + lane;
+                if (mk & (1u << lane)) {
+                    ms.flag[i] = 1;
+                    if (member_out) member_out[s_r[i]] = c;
+                }
+                while (mk) {
+                    int ii = ch * 32 + __ffs(mk) - 1;
+                    mk &= mk - 1;
                     if (lane < 21) {
+                        T w = s_w[ii];
                         T mu[6];
                         src.mean(s_r[ii], mu);
                         const T* cv = src.cov(s_r[ii]);
@@ -606,36 +719,34 @@ __device__ int merge_loop(const Src& src, const T* s_w, const int* s_r, int n, T
                         accc += w * (cv[lane] + da * db);
                     }
                 }
-                if (i < n && s_flag[i] == 2) {
-                    s_flag[i] = 1;
-                    if (member_out) member_out[s_r[i]] = n_out;
-                }
             }
-            if (lane < 21) s_acc[7 + lane] = accc / W;
+            const T my_cov = (lane < 21) ? accc / W : T(0);
+            T row[28];
+            row[0] = W;
+#pragma unroll
+            for (int a = 0; a < 6; ++a) row[1 + a] = mean[a];
+#pragma unroll
+            for (int q = 0; q < 21; ++q) row[7 + q] = __shfl_sync(0xffffffffu, my_cov, q);
+            T L[21];
+            const bool pd = chol6(row + 7, L);
+            T* o = sparse + (size_t)c * kRow;
+            if (lane < 28) {
+                T v;
+                if (pd) v = row[0];
+                else v = s_w[c];   // "bad hack, just keep the max feature" (kernels.cu:855-862)
+#pragma unroll
+                for (int q = 1; q < 28; ++q)
+                    if (lane == q) v = pd ? row[q] : (q < 7 ? cmu[q - 1] : ccov[q - 7]);
+                o[lane] = v;
+            }
+            if (lane == 0) ms.is_center[c] = 1;
             __syncwarp();
-            if (lane == 0) {
-                T row[kRow];
-                row[0] = W;
-                for (int a = 0; a < 6; ++a) row[1 + a] = mean[a];
-                for (int i = 0; i < 21; ++i) row[7 + i] = s_acc[7 + i];
-                T L[21];
-                bool pd = chol6(row + 7, L);
-                T* o = out + (size_t)n_out * kRow;
-                if (n_out < out_cap) {
-                    if (pd) {
-                        for (int i = 0; i < 28; ++i) o[i] = row[i];
-                    } else {   // "bad hack, just keep the max feature" (kernels.cu:855-862)
-                        o[0] = s_w[c];
-                        for (int a = 0; a < 6; ++a) o[1 + a] = s_cmu[a];
-                        for (int i = 0; i < 21; ++i) o[7 + i] = s_ccov[i];
-                    }
-                }
-            }
         }
-        ++n_out;
-        __syncthreads();
     }
-    return n_out;
+    atomicAdd(&s_evals, evals);
+    __syncthreads();
+    if (tid == 0 && counters) atomicAdd(&counters[12], (unsigned long long)s_evals);
+    return s_stop;
 }
 
 template <typename T, int K>
@@ -645,13 +756,21 @@ __global__ void __launch_bounds__(128) k_merge(Params prm, Bufs<T> b, int cur, i
     const int tid = threadIdx.x;
     const int G = b.map_n[cur][b.src[p]];
     const int n = min(b.surv_n[p], prm.Scap);
+    const int S2 = 2 * prm.Scap + 2 * prm.Gcap;   // sort capacity (survivors, then map entries)
     int n_pad = 1;
     while (n_pad < n) n_pad <<= 1;
     T* s_w = reinterpret_cast<T*>(smem);
-    uint32_t* s_key = reinterpret_cast<uint32_t*>(s_w + 2 * prm.Scap);
-    int* s_r = reinterpret_cast<int*>(s_key + 2 * prm.Scap);
-    T* s_pf = reinterpret_cast<T*>(s_r + 2 * prm.Scap);
-    uint8_t* s_flag = reinterpret_cast<uint8_t*>(s_pf + 6 * prm.Scap);
+    uint32_t* s_key = reinterpret_cast<uint32_t*>(s_w + S2);
+    int* s_r = reinterpret_cast<int*>(s_key + S2);
+    T* s_pf = reinterpret_cast<T*>(s_r + S2);
+    int* s_uf = reinterpret_cast<int*>(s_pf + 6 * prm.Scap);
+    int* s_roots = s_uf + prm.Scap;
+    int* s_pos = s_roots + prm.Scap;                              // Scap + Gcap
+    uint32_t* s_masks = reinterpret_cast<uint32_t*>(s_pos + prm.Scap + prm.Gcap);
+    const int nchunk = (prm.Scap + 31) / 32;
+    uint8_t* s_flag = reinterpret_cast<uint8_t*>(s_masks + (blockDim.x / 32) * nchunk);
+    uint8_t* s_cent = s_flag + prm.Scap;
+    __shared__ int s_tmp[40];
     for (int i = tid; i < n_pad; i += blockDim.x) {
         if (i < n) {
             s_w[i] = b.surv_w[(size_t)p * prm.Scap + i];
@@ -689,95 +808,88 @@ __global__ void __launch_bounds__(128) k_merge(Params prm, Bufs<T> b, int cur, i
     src.bcov[tri(3, 3)] = (T)prm.var_vu0;
     src.bcov[tri(4, 4)] = (T)prm.var_vv0;
     src.bcov[tri(5, 5)] = (T)prm.var_vd0;
-    T* out = b.merged + (size_t)p * prm.Scap * kRow;
+    T* sparse = b.mtmp + (size_t)p * prm.Scap * kRow;
     const T margin = sizeof(T) == 4 ? T(1.05) : T(1.000001);
-    int n_out = merge_loop<T>(src, s_w, s_r, n, s_pf, s_flag, (T)prm.min_sep, margin, out, prm.Scap, nullptr);
-    // new map: merged components then retained non-detection clouds (.cu:1923-2058)
-    __shared__ int s_nnd, s_total;
+    MergeScratch<T> ms{s_pf, s_flag, s_cent, s_uf, s_roots, s_masks, nchunk};
+    const int stop = merge_components<T>(src, s_w, s_r, n, ms, (T)prm.min_sep, margin, sparse, nullptr,
+                                         b.counters);
+    // merged list in centre order (centres after a stop are dropped, as the reference's loop ends there)
+    for (int i = tid; i < n; i += blockDim.x) s_pos[i] = (i < stop && s_cent[i]) ? 1 : 0;
     __syncthreads();
-    if (tid == 0) {
-        int nnd = 0;
-        for (int j = 0; j < G; ++j) {
-            const T* fr = b.fit + ((size_t)p * prm.Gcap + j) * kRow;
-            T wnd = fr[0] * (T(1) - fr[1]);
-            nnd += wnd >= (T)prm.min_weight;
+    const int n_out = block_exclusive_scan(s_pos, n, s_tmp);
+    T* out = b.merged + (size_t)p * prm.Scap * kRow;
+    for (int i = tid; i < n; i += blockDim.x) {
+        if (i < stop && s_cent[i]) {
+            const T* sr = sparse + (size_t)i * kRow;
+            T* dr = out + (size_t)s_pos[i] * kRow;
+            for (int q = 0; q < 28; ++q) dr[q] = sr[q];
         }
-        s_nnd = nnd;
-        s_total = n_out + nnd;
-        b.merged_n[p] = n_out;
     }
     __syncthreads();
-    const int total = s_total;
-    T thr = T(-1);   // keep every entry with weight > thr, and ties in order, up to Gcap
-    int n_ties_keep = 0x7fffffff;
-    if (total > prm.Gcap) {
-        // weight threshold: the Gcap-th largest weight among all entries
-        if (tid == 0) {
-            atomicAdd(&b.counters[0], 1ull);
+    // new map: merged components then retained non-detection clouds (.cu:1923-2058);
+    // entries e < n_out are merged, e >= n_out are the Gaussians j = e - n_out
+    const T minw = (T)prm.min_weight;
+    const int n_all = n_out + G;
+    for (int e = tid; e < n_all; e += blockDim.x) {
+        T w;
+        if (e < n_out) {
+            w = out[(size_t)e * kRow];
+        } else {
+            const T* fr = b.fit + ((size_t)p * prm.Gcap + (e - n_out)) * kRow;
+            T wnd = fr[0] * (T(1) - fr[1]);
+            w = (wnd >= minw) ? wnd : T(-1);   // -1: not retained
         }
-        __shared__ T s_thr;
-        __shared__ int s_tie;
-        if (tid == 0) {
-            // bisection over the weight value
-            T lo = 0, hi = 0;
-            for (int i = 0; i < n_out; ++i) hi = max(hi, out[(size_t)i * kRow]);
-            for (int j = 0; j < G; ++j) {
-                const T* fr = b.fit + ((size_t)p * prm.Gcap + j) * kRow;
-                T wnd = fr[0] * (T(1) - fr[1]);
-                if (wnd >= (T)prm.min_weight) hi = max(hi, wnd);
-            }
-            for (int it = 0; it < 60; ++it) {
-                T mid = (lo + hi) / 2;
-                int cnt = 0;
-                for (int i = 0; i < n_out; ++i) cnt += out[(size_t)i * kRow] > mid;
-                for (int j = 0; j < G; ++j) {
-                    const T* fr = b.fit + ((size_t)p * prm.Gcap + j) * kRow;
-                    T wnd = fr[0] * (T(1) - fr[1]);
-                    cnt += (wnd >= (T)prm.min_weight) && wnd > mid;
-                }
-                if (cnt >= prm.Gcap) lo = mid; else hi = mid;
-            }
-            int above = 0;
-            for (int i = 0; i < n_out; ++i) above += out[(size_t)i * kRow] > hi;
-            for (int j = 0; j < G; ++j) {
-                const T* fr = b.fit + ((size_t)p * prm.Gcap + j) * kRow;
-                T wnd = fr[0] * (T(1) - fr[1]);
-                above += (wnd >= (T)prm.min_weight) && wnd > hi;
-            }
-            s_thr = hi;
-            s_tie = prm.Gcap - above;
+        s_w[e] = w;
+        s_pos[e] = w >= T(0) ? 1 : 0;
+    }
+    __syncthreads();
+    int total = block_exclusive_scan(s_pos, n_all, s_tmp);
+    if (total > prm.Gcap) {
+        // keep the Gcap largest weights (ties in entry order): sort copies of the weights
+        int np2 = 1;
+        while (np2 < n_all) np2 <<= 1;
+        for (int e = tid; e < np2; e += blockDim.x) {
+            s_key[e] = (uint32_t)e;
+            s_r[e] = e;
+            if (e >= n_all) s_w[e] = T(-2);
         }
         __syncthreads();
-        thr = s_thr;
-        n_ties_keep = s_tie;
+        sort_survivors(s_w, s_key, s_r, np2);   // descending weight, then entry order
+        for (int e = tid; e < n_all; e += blockDim.x) s_pos[e] = 0;
+        __syncthreads();
+        for (int e = tid; e < prm.Gcap; e += blockDim.x)
+            if (s_w[e] >= T(0)) s_pos[s_r[e]] = 1;
+        __syncthreads();
+        if (tid == 0) atomicAdd(&b.counters[0], 1ull);
+        total = block_exclusive_scan(s_pos, n_all, s_tmp);
     }
+    // write the kept entries in entry order
     const int wrow = p;   // the new map lives at row p of the other buffer
-    if (tid == 0) {
-        int k = 0, ties = 0;
-        T* mo = b.map[cur ^ 1] + (size_t)wrow * prm.Gcap * kRow;
-        int* mr = b.map_ref[cur ^ 1] + (size_t)wrow * prm.Gcap;
-        for (int i = 0; i < n_out && k < prm.Gcap; ++i) {
-            T w = out[(size_t)i * kRow];
-            bool keep = total <= prm.Gcap || w > thr || (w == thr && ties++ < n_ties_keep);
-            if (!keep) continue;
-            for (int q = 0; q < 28; ++q) mo[(size_t)k * kRow + q] = out[(size_t)i * kRow + q];
-            mr[k] = -1 - i;
-            ++k;
-        }
-        for (int j = 0; j < G && k < prm.Gcap; ++j) {
+    T* mo = b.map[cur ^ 1] + (size_t)wrow * prm.Gcap * kRow;
+    int* mr = b.map_ref[cur ^ 1] + (size_t)wrow * prm.Gcap;
+    for (int e = tid; e < n_all; e += blockDim.x) {
+        const int pos = s_pos[e];
+        const int nxt = (e + 1 < n_all) ? s_pos[e + 1] : total;
+        if (nxt == pos) continue;   // not kept
+        if (e < n_out) {
+            const T* sr = out + (size_t)e * kRow;
+            for (int q = 0; q < 28; ++q) mo[(size_t)pos * kRow + q] = sr[q];
+            mr[pos] = -1 - e;
+        } else {
+            const int j = e - n_out;
             const T* fr = b.fit + ((size_t)p * prm.Gcap + j) * kRow;
-            T wnd = fr[0] * (T(1) - fr[1]);
-            if (!(wnd >= (T)prm.min_weight)) continue;
-            bool keep = total <= prm.Gcap || wnd > thr || (wnd == thr && ties++ < n_ties_keep);
-            if (!keep) continue;
-            mo[(size_t)k * kRow] = wnd;
-            mr[k] = p * prm.Gcap + j;
-            ++k;
+            mo[(size_t)pos * kRow] = fr[0] * (T(1) - fr[1]);
+            mr[pos] = p * prm.Gcap + j;
         }
-        b.map_n[cur ^ 1][wrow] = k;
+    }
+    if (tid == 0) {
+        b.merged_n[p] = n_out;
+        b.map_n[cur ^ 1][wrow] = total;
         double* me = b.map_ext[cur ^ 1] + 12 * wrow;
         for (int q = 0; q < 12; ++q) me[q] = fixed ? 0.0 : b.ext[12 * p + q];
         atomicAdd(&b.counters[5], (unsigned long long)n);
+        atomicAdd(&b.counters[7], (unsigned long long)n);
+        atomicAdd(&b.counters[11], (unsigned long long)n_out);
     }
 }
 
@@ -1003,12 +1115,12 @@ __global__ void __launch_bounds__(256) k_materialize(Params prm, Bufs<T> b, int 
 }
 
 // ---------------------------------------------------------------- stand-alone merge
+// phdUpdateMergeKernel on an explicit component list (rows of kRow) with prune flags.
 template <typename T>
 __global__ void __launch_bounds__(128) k_merge_list(const T* rows, const uint8_t* flags_in, int n_all,
-                                                    T min_sep, T* out, int* n_out_p, int* member_of) {
+                                                    T min_sep, T* sparse, T* out, int* n_out_p, int* member_of) {
     extern __shared__ __align__(16) unsigned char smem[];
-    // survivors = unflagged inputs, sorted by the argmax order
-    __shared__ int s_n;
+    __shared__ int s_n, s_tmp[40];
     if (threadIdx.x == 0) {
         int n = 0;
         for (int i = 0; i < n_all; ++i) n += !flags_in[i];
@@ -1018,11 +1130,18 @@ __global__ void __launch_bounds__(128) k_merge_list(const T* rows, const uint8_t
     const int n = s_n;
     int n_pad = 1;
     while (n_pad < n) n_pad <<= 1;
+    const int cap = n_all + 1;
     T* s_w = reinterpret_cast<T*>(smem);
-    uint32_t* s_key = reinterpret_cast<uint32_t*>(s_w + 2 * n_all + 2);
-    int* s_r = reinterpret_cast<int*>(s_key + 2 * n_all + 2);
-    T* s_pf = reinterpret_cast<T*>(s_r + 2 * n_all + 2);
-    uint8_t* s_flag = reinterpret_cast<uint8_t*>(s_pf + 6 * n_all + 6);
+    uint32_t* s_key = reinterpret_cast<uint32_t*>(s_w + 2 * cap);
+    int* s_r = reinterpret_cast<int*>(s_key + 2 * cap);
+    T* s_pf = reinterpret_cast<T*>(s_r + 2 * cap);
+    int* s_uf = reinterpret_cast<int*>(s_pf + 6 * cap);
+    int* s_roots = s_uf + cap;
+    int* s_pos = s_roots + cap;
+    const int nchunk = (cap + 31) / 32;
+    uint32_t* s_masks = reinterpret_cast<uint32_t*>(s_pos + cap);
+    uint8_t* s_flag = reinterpret_cast<uint8_t*>(s_masks + (blockDim.x / 32) * nchunk);
+    uint8_t* s_cent = s_flag + cap;
     if (threadIdx.x == 0) {
         int k = 0;
         for (int i = 0; i < n_all; ++i)
@@ -1038,8 +1157,21 @@ __global__ void __launch_bounds__(128) k_merge_list(const T* rows, const uint8_t
     sort_survivors(s_w, s_key, s_r, n_pad);
     ListSource<T> src{rows};
     const T margin = sizeof(T) == 4 ? T(1.05) : T(1.000001);
-    // membership: rerun the marking through a per-survivor record of the output row
-    int n_out = merge_loop<T>(src, s_w, s_r, n, s_pf, s_flag, min_sep, margin, out, n_all, member_of);
+    MergeScratch<T> ms{s_pf, s_flag, s_cent, s_uf, s_roots, s_masks, nchunk};
+    const int stop = merge_components<T>(src, s_w, s_r, n, ms, min_sep, margin, sparse, member_of, nullptr);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s_pos[i] = (i < stop && s_cent[i]) ? 1 : 0;
+    __syncthreads();
+    const int n_out = block_exclusive_scan(s_pos, n, s_tmp);
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        if (i < stop && s_cent[i])
+            for (int q = 0; q < 28; ++q) out[(size_t)s_pos[i] * kRow + q] = sparse[(size_t)i * kRow + q];
+    __syncthreads();
+    // membership: centre index -> output row
+    if (member_of)
+        for (int i = threadIdx.x; i < n_all; i += blockDim.x) {
+            int c = member_of[i];
+            member_of[i] = (c >= 0 && c < stop) ? s_pos[c] : -1;
+        }
     if (threadIdx.x == 0) *n_out_p = n_out;
 }
 

@@ -149,6 +149,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "scphd_update_device": (i32, [vp, vp, vp, vp, i32, i32]),
         "scphd_resample": (i32, [vp, P(i32)]),
         "scphd_step": (i32, [vp, d, P(d), P(d), P(d), i32, i32]),
+        "scphd_step_device": (i32, [vp, d, vp, vp, vp, i32, i32]),
         "scphd_check": (i32, [vp]),
         "scphd_synchronize": (i32, [vp]),
         "scphd_get_particles": (i32, [vp, P(d), P(d)]),
@@ -162,6 +163,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "scphd_get_counters": (i32, [vp, P(i64)]),
         "scphd_merge_components": (i32, [P(d), P(u8), i32, d, i32, P(d), P(i32), P(i32)]),
         "scphd_systematic_resample": (i32, [P(d), i32, d, P(i32)]),
+        "scphd_stream": (vp, [vp]),
+        "scphd_set_profiling": (i32, [vp, i32]),
+        "scphd_get_stage_times": (i32, [vp, P(d), P(i64)]),
         "scphd_last_error": (ctypes.c_char_p, []),
         "scphd_kernel_launches": (i64, []),
     }
@@ -263,6 +267,14 @@ class SCPHDCameraCalibration:
         _check(self._lib.scphd_step(self._h, float(dt), _dptr(u), _dptr(v), _dptr(dd),
                                     int(u.size), int(bool(fixed_camera))))
 
+    def step_device(self, dt: float, u_ptr: int, v_ptr: int, d_ptr: Optional[int], n: int,
+                    fixed_camera: bool = False) -> None:
+        """predict + update + resample with device-resident FP64 measurement vectors;
+        no host synchronisation."""
+        _check(self._lib.scphd_step_device(self._h, float(dt), ctypes.c_void_p(u_ptr), ctypes.c_void_p(v_ptr),
+                                           ctypes.c_void_p(d_ptr) if d_ptr else None, int(n),
+                                           int(bool(fixed_camera))))
+
     def checkStuff(self) -> None:
         _check(self._lib.scphd_check(self._h))
 
@@ -318,9 +330,26 @@ class SCPHDCameraCalibration:
         return idx
 
     def counters(self) -> np.ndarray:
-        c = np.zeros(8, np.int64)
+        c = np.zeros(16, np.int64)
         _check(self._lib.scphd_get_counters(self._h, c.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
         return c
+
+    @property
+    def stream_handle(self) -> int:
+        """cudaStream_t of the handle (an integer), e.g. for torch.cuda.ExternalStream."""
+        return int(self._lib.scphd_stream(self._h) or 0)
+
+    def set_profiling(self, enable: bool) -> None:
+        _check(self._lib.scphd_set_profiling(self._h, int(bool(enable))))
+
+    STAGES = ("predict_parents", "cloud_fit", "likelihood", "merge", "weights", "resample")
+
+    def stage_times(self):
+        """{stage: (total ms, launches)} since the last call (profiling mode)."""
+        ms = np.zeros(8, np.float64)
+        n = np.zeros(8, np.int64)
+        _check(self._lib.scphd_get_stage_times(self._h, _dptr(ms), n.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
+        return {name: (float(ms[i]), int(n[i])) for i, name in enumerate(self.STAGES)}
 
     def set_state(self, states, log_weights, sizes, weights, clouds, omega) -> None:
         states, log_weights = _f64(states), _f64(log_weights)
