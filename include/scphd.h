@@ -195,6 +195,27 @@ scphd_status scphd_merge_components(const double* comps, const uint8_t* flags, i
                                     double min_separation, int32_t precision,
                                     double* merged, int32_t* n_out, int32_t* member_of);
 
+/* scphd_merge_components_static: the same greedy merge as scphd_merge_components,
+ * for callers that must not allocate device memory — a host that runs inside
+ * another framework's memory pool (which owns all free device memory, so a
+ * cudaMalloc can fail), or a latency-bounded loop (cudaMalloc and cudaFree can
+ * synchronise the device and stall behind unrelated work).  It calls no
+ * cudaMalloc, cudaFree or other allocating routine: its device scratch (inputs,
+ * outputs and working rows, about 0.6 MB) is one static array that every GPU
+ * loading this library holds until the process exits.  Limits and sharing:
+ * n <= SCPHD_STATIC_MERGE_MAX components (larger n returns SCPHD_ERR_CAPACITY);
+ * every call on a device uses the same array, so calls that overlap on the GPU
+ * (from several host threads) race and must be serialised by the caller; the
+ * array keeps the previous call's contents, and the call re-initialises what it
+ * reads.  The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call before
+ * any stream capture.  Arguments, outputs and errors as scphd_merge_components.
+ * This entry point has no counterpart in the reference. */
+#define SCPHD_STATIC_MERGE_MAX 512
+scphd_status scphd_merge_components_static(const double* comps, const uint8_t* flags, int32_t n,
+                                           double min_separation, int32_t precision,
+                                           double* merged, int32_t* n_out, int32_t* member_of);
+
 /* scphd_systematic_resample: the systematic resampling of resample()
  * (src/scphdcameracalibration.cu:2660-2702) on n linear weights with the offset
  * u01 * (1/n); writes n indices. */

@@ -8,6 +8,7 @@
 
 #include <atomic>
 #include <cmath>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -817,6 +818,124 @@ scphd_status scphd_merge_components(const double* comps, const uint8_t* flags, i
     };
     (void)dev;
     return precision == SCPHD_FP64 ? run(double()) : run(float());
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free merge: all device buffers of one call live in one static
+// device array.  Layout (bytes, each part 256-aligned): host input rows as FP64
+// (n x 28), prune flags (n), working rows in T (n x kRow), merge output indexed
+// by centre (n x kRow), compact output (n x kRow), output converted to FP64
+// (n x 28), membership (n int32), output count (int32).  Sized for T = double.
+}  // extern "C"
+
+namespace {
+
+constexpr int kStaticMax = SCPHD_STATIC_MERGE_MAX;
+constexpr size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr size_t kOffIn = 0;
+constexpr size_t kOffFlags = kOffIn + al256((size_t)kStaticMax * 28 * 8);
+constexpr size_t kOffRows = kOffFlags + al256(kStaticMax);
+constexpr size_t kOffSparse = kOffRows + al256((size_t)kStaticMax * kRow * 8);
+constexpr size_t kOffOut = kOffSparse + al256((size_t)kStaticMax * kRow * 8);
+constexpr size_t kOffOut28 = kOffOut + al256((size_t)kStaticMax * kRow * 8);
+constexpr size_t kOffMember = kOffOut28 + al256((size_t)kStaticMax * 28 * 8);
+constexpr size_t kOffCount = kOffMember + al256((size_t)kStaticMax * 4);
+constexpr size_t kStaticBytes = kOffCount + 256;
+
+// Device-side scratch of scphd_merge_components_static.  In host code this name is
+// only a stand-in for the symbol: the device address comes from
+// cudaGetSymbolAddress (static_scratch_ptr below).
+static __device__ __align__(256) unsigned char g_static_merge_scratch[kStaticBytes];
+
+std::mutex g_static_mu;
+void* g_static_ptr[256] = {nullptr};
+
+// the array's device address on the current device, looked up once per device
+scphd_status static_scratch_ptr(unsigned char** out) {
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) return fail(SCPHD_ERR_INVALID, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_merge_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(SCPHD_ERR_CUDA, std::string("cudaGetSymbolAddress(static merge scratch): ") +
+                                            cudaGetErrorString(e));
+        g_static_ptr[dev] = p;
+    }
+    *out = static_cast<unsigned char*>(g_static_ptr[dev]);
+    return SCPHD_OK;
+}
+
+template <typename T> __global__ void k_rows_from28(const double* in, int n, T* rows) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * kRow) return;
+    int r = i / kRow, q = i - r * kRow;
+    rows[i] = q < 28 ? (T)in[(size_t)r * 28 + q] : T(0);
+}
+
+template <typename T> __global__ void k_rows_to28(const T* rows, const int* count, double* out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= *count * 28) return;
+    int r = i / 28, q = i - r * 28;
+    out[i] = (double)rows[(size_t)r * kRow + q];
+}
+
+template <typename T>
+scphd_status merge_static_impl(unsigned char* base, const double* comps, const uint8_t* flags, int n,
+                               double min_separation, double* merged, int32_t* n_out, int32_t* member_of) {
+    double* d_in = reinterpret_cast<double*>(base + kOffIn);
+    uint8_t* d_flags = reinterpret_cast<uint8_t*>(base + kOffFlags);
+    T* d_rows = reinterpret_cast<T*>(base + kOffRows);
+    T* d_sparse = reinterpret_cast<T*>(base + kOffSparse);
+    T* d_out = reinterpret_cast<T*>(base + kOffOut);
+    double* d_out28 = reinterpret_cast<double*>(base + kOffOut28);
+    int* d_mem = reinterpret_cast<int*>(base + kOffMember);
+    int* d_cnt = reinterpret_cast<int*>(base + kOffCount);
+    CUDA_TRY(cudaMemcpy(d_in, comps, sizeof(double) * 28 * (size_t)n, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(d_flags, flags, (size_t)n, cudaMemcpyHostToDevice));
+    // the array keeps the previous call's contents: membership must start at -1
+    CUDA_TRY(cudaMemset(d_mem, 0xff, sizeof(int) * (size_t)n));
+    k_rows_from28<T><<<(n * kRow + 255) / 256, 256>>>(d_in, n, d_rows);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    const size_t cap = (size_t)n + 1, nchunk = (cap + 31) / 32;
+    const size_t smem = 2 * cap * (sizeof(T) + 8) + 6 * cap * sizeof(T) + 3 * cap * 4 + 4 * nchunk * 4 + 2 * cap + 64;
+    CUDA_TRY(cudaFuncSetAttribute(k_merge_list<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_merge_list<T><<<1, 128, smem>>>(d_rows, d_flags, n, (T)min_separation, d_sparse, d_out, d_cnt, d_mem);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    k_rows_to28<T><<<(n * 28 + 255) / 256, 256>>>(d_out, d_cnt, d_out28);
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    CUDA_TRY(cudaGetLastError());
+    int cnt = 0;
+    CUDA_TRY(cudaMemcpy(&cnt, d_cnt, sizeof(int), cudaMemcpyDeviceToHost));
+    if (cnt < 0 || cnt > n) return fail(SCPHD_ERR_CUDA, "static merge returned an invalid count");
+    if (cnt) CUDA_TRY(cudaMemcpy(merged, d_out28, sizeof(double) * 28 * (size_t)cnt, cudaMemcpyDeviceToHost));
+    if (member_of) CUDA_TRY(cudaMemcpy(member_of, d_mem, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost));
+    *n_out = cnt;
+    return SCPHD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+scphd_status scphd_merge_components_static(const double* comps, const uint8_t* flags, int32_t n,
+                                           double min_separation, int32_t precision, double* merged,
+                                           int32_t* n_out, int32_t* member_of) {
+    if (n < 0 || (n > 0 && (!comps || !flags || !merged || !n_out))) return fail(SCPHD_ERR_INVALID, "bad arguments");
+    if (n > kStaticMax)
+        return fail(SCPHD_ERR_CAPACITY, "scphd_merge_components_static takes at most " +
+                                            std::to_string(kStaticMax) + " components, got " + std::to_string(n));
+    if (!(min_separation > 0)) return fail(SCPHD_ERR_INVALID, "min_separation must be > 0");
+    if (precision != SCPHD_FP32 && precision != SCPHD_FP64) return fail(SCPHD_ERR_INVALID, "bad precision");
+    if (n_out) *n_out = 0;
+    if (n == 0) return SCPHD_OK;
+    unsigned char* base = nullptr;
+    scphd_status s = static_scratch_ptr(&base);
+    if (s != SCPHD_OK) return s;
+    return precision == SCPHD_FP64 ? merge_static_impl<double>(base, comps, flags, n, min_separation, merged, n_out, member_of)
+                                   : merge_static_impl<float>(base, comps, flags, n, min_separation, merged, n_out, member_of);
 }
 
 scphd_status scphd_systematic_resample(const double* weights, int32_t n, double u01v, int32_t* idx) {
