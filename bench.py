@@ -113,6 +113,25 @@ def dist_env():
     return world, rank, local
 
 
+def combine_ranks(ms_total: float, units: float, e2e_ms: float, e2e_units: float, dist=None, device=None):
+    """Whole-job figures over the ranks of a replica run: device times take the MAX
+    over ranks (the job ends with its slowest rank), units the SUM.  Works with any
+    torch.distributed backend (NCCL on GPUs, gloo in the CPU tests)."""
+    import torch
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return ms_total, units, e2e_ms, e2e_units
+    t = torch.tensor([ms_total, units, e2e_ms, e2e_units], dtype=torch.float64, device=device)
+    mx, sm = t.clone(), t.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return mx[0].item(), sm[1].item(), mx[2].item(), sm[3].item()
+
+
+def replica_seed_index(rank: int) -> int:
+    """Filter index of a rank's replica: each rank runs its own seeded scene."""
+    return rank
+
+
 def cpu_oracle_rate(pkg, workload: str, sample_parents: int, prefill: int, frames: int, threads: int):
     """Units/s of the FP64 oracle (the CPU restatement of the reference) on a
     bounded sample of the workload: the same scene with `sample_parents` parents."""
@@ -199,7 +218,8 @@ def run_b200(args):
     prec = pkg.SCPHD_FP32 if args.precision == "fp32" else pkg.SCPHD_FP64
     K, W = args.steps, args.warmup
     n_frames = args.prefill + W + 3 * K + 1
-    sc, cfg = pkg.scene.workload(args.workload, precision=prec, filter_index=rank, n_frames=n_frames)
+    sc, cfg = pkg.scene.workload(args.workload, precision=prec, filter_index=replica_seed_index(rank),
+                                 n_frames=n_frames)
     if args.parents:
         cfg.n_parents = args.parents   # smaller case for profiler captures; not a bench line
     cfg.device = local
@@ -272,15 +292,8 @@ def run_b200(args):
     e2e_ms = ee0.elapsed_time(ee1)
     e2e_units = int(ce1[6] - ce0[6])
 
-    tot = torch.tensor([ms_total, float(units), e2e_ms, float(e2e_units)], dtype=torch.float64, device=dev)
-    if dist:
-        mx = tot.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = tot.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        ms_all, units_all, e2e_ms_all, e2e_units_all = mx[0].item(), sm[1].item(), mx[2].item(), sm[3].item()
-    else:
-        ms_all, units_all, e2e_ms_all, e2e_units_all = ms_total, float(units), e2e_ms, float(e2e_units)
+    ms_all, units_all, e2e_ms_all, e2e_units_all = combine_ranks(ms_total, float(units), e2e_ms,
+                                                                 float(e2e_units), dist, dev)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -347,7 +360,8 @@ def run_b200(args):
         "stage_ms_per_frame": {k2: v[0] / max(1, v[1]) for k2, v in stages.items()},
         "cpu_baseline": cpu,
         "clocks": clk,
-        "counters": {"truncations": int(c1[0]), "scratch_overflows": int(c1[1])},
+        "counters": {"map_truncations": int(c1[0] - c0[0]), "scratch_overflows": int(c1[1]),
+                     "max_survivors_per_parent": int(c1[13]), "max_survivors_capacity": int(cfg.max_survivors)},
     }
     print(json.dumps(line), flush=True)
     filt.close()

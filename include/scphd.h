@@ -168,7 +168,8 @@ scphd_status scphd_set_state(scphd_filter* f, const double* states, const double
  * [5] survivors of the last update (sum over parents), [6] units since create,
  * [7] survivors since create, [8] sample clouds read from memory, [9] sample
  * clouds written, [10] Gaussians fitted, [11] merged components produced,
- * [12] full Mahalanobis evaluations in the merge; [13..15] reserved. */
+ * [12] full Mahalanobis evaluations in the merge, [13] largest survivor count of
+ * one parent (before the max_survivors cut); [14..15] reserved. */
 scphd_status scphd_get_counters(scphd_filter* f, int64_t counters[16]);
 
 /* The CUDA stream (a cudaStream_t) all of the handle's work is issued on, so a

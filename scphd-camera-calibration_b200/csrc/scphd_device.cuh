@@ -83,6 +83,34 @@ template <> struct Normals<float> {
     }
 };
 
+// One Box-Muller pair from two 32-bit words: z0 = r cos(2 pi u_b), z1 = r sin(2 pi u_b),
+// r = sqrt(-2 log u_a), the same pair Normals<T>::four produces.  The FP32 form uses
+// the MUFU approximations (lg2, sin, cos) with the angle shifted into [-pi, pi):
+// cos(2 pi u) = -cos(2 pi (u - 1/2)), sin likewise.
+template <typename T> struct Pair;
+template <> struct Pair<double> {
+    __device__ static void two(uint32_t wa, uint32_t wb, double& z0, double& z1) {
+        double r = sqrt(-2.0 * log(u01(wa)));
+        double s, c;
+        sincos((2.0 * 3.14159265358979323846) * u01(wb), &s, &c);
+        z0 = r * c;
+        z1 = r * s;
+    }
+};
+template <> struct Pair<float> {
+    __device__ static void two(uint32_t wa, uint32_t wb, float& z0, float& z1) {
+        float ua = __fmaf_rn((float)wa, 0x1p-32f, 0x1p-33f);
+        float ub = __fmaf_rn((float)wb, 0x1p-32f, 0x1p-33f);
+        ua = fminf(ua, 0.99999994f);
+        float r = sqrtf(-2.0f * __logf(ua));
+        float th = 6.283185307179586f * (ub - 0.5f);
+        float s, c;
+        __sincosf(th, &s, &c);
+        z0 = -r * c;
+        z1 = -r * s;
+    }
+};
+
 template <typename T> __device__ __forceinline__ T tsqrt(T x);
 template <> __device__ __forceinline__ float tsqrt(float x) { return sqrtf(x); }
 template <> __device__ __forceinline__ double tsqrt(double x) { return sqrt(x); }
@@ -244,12 +272,18 @@ __device__ inline T mahal6(const T* ma, const T* Sa, const T* mb, const T* Sb) {
 // Measurement-independent Kalman terms of one fitted Gaussian for H = [I_K 0],
 // R = diag(var): S^-1, log-constant c = log pD + log w - K/2 log 2pi - 1/2 log det S,
 // gain K = P H' S^-1 and the Joseph-form posterior covariance
-// (I - K H) P (I - K H)' + K R K' of computeDetectionsKernel
-// (src/kernels.cu:506-595), which does not depend on the measurement.
+// (I - K H) P (I - K H)' + K R K' of computeDetectionsKernel (src/kernels.cu:506-595),
+// which does not depend on the measurement.  Spread over a warp: every lane holds the fitted Gaussian (w, pD, packed
+// cov P); S, S^-1 and the log-constant are computed redundantly, the 18 gain entries
+// and the 21 Joseph-form covariance entries one per lane through the warp's shared
+// scratch sm (72 T), and the PD test of the posterior by every lane from shared
+// memory.  Writes the 47 prep values of this Gaussian to dst.
 template <typename T, int K>
-__device__ inline void kalman_prep(const T* fitrow, const Model& m, T* prep) {
-    const T w = fitrow[0], pdbar = fitrow[1];
-    const T* P = fitrow + 8;
+__device__ inline void warp_kalman_prep(T w, T pdbar, const T* P, const Model& m, T* sm, int lane, T* dst) {
+    T* sP = sm;          // 21
+    T* sSi = sm + 21;    // 6
+    T* sK = sm + 27;     // 18 (row-major 6 x 3)
+    T* sPn = sm + 45;    // 21
     T S[6], Si[6];
     S[0] = P[0] + (T)m.var[0];
     S[1] = P[1];
@@ -261,7 +295,6 @@ __device__ inline void kalman_prep(const T* fitrow, const Model& m, T* prep) {
         Si[3] = Si[4] = Si[5] = 0;
     } else {
         S[3] = P[3]; S[4] = P[4]; S[5] = P[5] + (T)m.var[2];
-        // packed: S00=S[0], S10=S[1], S11=S[2], S20=S[3], S21=S[4], S22=S[5]
         T a = S[0], b = S[1], c = S[2], d = S[3], e = S[4], f = S[5];
         T A00 = c * f - e * e, A10 = d * e - b * f, A11 = a * f - d * d;
         T A20 = b * e - c * d, A21 = b * d - a * e, A22 = a * c - b * b;
@@ -270,51 +303,62 @@ __device__ inline void kalman_prep(const T* fitrow, const Model& m, T* prep) {
         Si[3] = A20 / det; Si[4] = A21 / det; Si[5] = A22 / det;
     }
     const T log2pi = (T)1.8378770664093454835606594728112;
-    T c;
+    T cst;
     if (pdbar > T(0) && w > T(0) && det > T(0))
-        c = tlog(pdbar) + tlog(w) - T(0.5) * T(K) * log2pi - T(0.5) * tlog(det);
+        cst = tlog(pdbar) + tlog(w) - T(0.5) * T(K) * log2pi - T(0.5) * tlog(det);
     else
-        c = tneg_inf<T>();
-    // gain K[r][cc] = sum_a P[r][a] Si[a][cc]
-    T Kg[18];
+        cst = tneg_inf<T>();
+    // stage P and S^-1 in shared memory
+    {
+        T v = P[0];
 #pragma unroll
-    for (int r = 0; r < 6; ++r)
+        for (int i = 1; i < 21; ++i) if (lane == i) v = P[i];
+        if (lane < 21) sP[lane] = v;
+        T u = Si[0];
 #pragma unroll
-        for (int cc = 0; cc < 3; ++cc) {
-            T s = 0;
-            if (cc < K) {
+        for (int i = 1; i < 6; ++i) if (lane == i) u = Si[i];
+        if (lane < 6) sSi[lane] = u;
+    }
+    __syncwarp();
+    // gain entry q = r*3 + cc: K[r][cc] = sum_a P[r][a] S^-1[a][cc]
+    if (lane < 18) {
+        const int r = lane / 3, cc = lane - 3 * (lane / 3);
+        T acc = 0;
+        if (cc < K) {
 #pragma unroll
-                for (int a = 0; a < K; ++a) s += P[tri(r, a)] * Si[tri(a, cc)];
-            }
-            Kg[r * 3 + cc] = s;
+            for (int a = 0; a < K; ++a) acc += sP[tri(r, a)] * sSi[tri(a, cc)];
         }
-    // Joseph: P' = P - K(HP) - (HP)'K' + K (HPH') K' + K R K'
-    T Pn[21];
+        sK[lane] = acc;
+        dst[kPrepK + lane] = acc;
+    }
+    __syncwarp();
+    // Joseph entry e = (ea, eb): P - K(HP) - (HP)'K' + K(HPH')K' + K R K'
+    if (lane < 21) {
+        int ea = 0;
+        while ((ea + 1) * (ea + 2) / 2 <= lane) ++ea;
+        const int eb = lane - ea * (ea + 1) / 2;
+        T s = sP[lane];
 #pragma unroll
-    for (int a = 0; a < 6; ++a)
+        for (int k = 0; k < K; ++k) {
+            const T Kak = sK[ea * 3 + k], Kbk = sK[eb * 3 + k];
+            s -= Kak * sP[tri(k, eb)];
+            s -= sP[tri(ea, k)] * Kbk;
+            s += Kak * (T)m.var[k] * Kbk;
 #pragma unroll
-        for (int b = 0; b <= a; ++b) {
-            T s = P[tri(a, b)];
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-                s -= Kg[a * 3 + k] * P[tri(k, b)];
-                s -= P[tri(a, k)] * Kg[b * 3 + k];
-                s += Kg[a * 3 + k] * (T)m.var[k] * Kg[b * 3 + k];
-#pragma unroll
-                for (int l = 0; l < K; ++l) s += Kg[a * 3 + k] * P[tri(k, l)] * Kg[b * 3 + l];
-            }
-            Pn[tri(a, b)] = s;
+            for (int l = 0; l < K; ++l) s += Kak * sP[tri(k, l)] * sK[eb * 3 + l];
         }
+        sPn[lane] = s;
+        dst[kPrepCov + lane] = s;
+    }
+    __syncwarp();
     T L[21];
-    bool pdok = chol6(Pn, L);
-    prep[0] = c;
-    prep[1] = pdok ? T(1) : T(0);
-#pragma unroll
-    for (int i = 0; i < 6; ++i) prep[kPrepSi + i] = Si[i];
-#pragma unroll
-    for (int i = 0; i < 18; ++i) prep[kPrepK + i] = Kg[i];
-#pragma unroll
-    for (int i = 0; i < 21; ++i) prep[kPrepCov + i] = Pn[i];
+    const bool pdok = chol6(sPn, L);
+    if (lane == 0) {
+        dst[0] = cst;
+        dst[1] = pdok ? T(1) : T(0);
+    }
+    if (lane < 6) dst[kPrepSi + lane] = sSi[lane];
+    __syncwarp();
 }
 
 // log-likelihood exponent term c - 1/2 nu' S^-1 nu for measurement z

@@ -224,11 +224,10 @@ public:
         a.cap = probe.used;
         carve(a);
         CUDA_TRY(cudaMemsetAsync(p, 0, probe.used, stream));
-        {
-            const size_t S = prm.Scap, G = prm.Gcap, S2 = 2 * S + 2 * G, nchunk = (S + 31) / 32;
-            merge_smem = S2 * (sizeof(T) + 8) + 6 * S * sizeof(T) + 2 * S * 4 + (S + G) * 4 + 4 * nchunk * 4 +
-                         2 * S + 64;
-        }
+        merge_smem = merge_smem_bytes<T>(prm.Scap, prm.Gcap, 4);
+        if (merge_smem > 227 * 1024)
+            return fail(SCPHD_ERR_CAPACITY, "max_survivors/max_gaussians need " + std::to_string(merge_smem) +
+                                                " bytes of shared memory per merge block (limit 227 KB)");
         if (prm.K == 2) {
             CUDA_TRY(cudaFuncSetAttribute(k_merge<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem));
         } else {
@@ -776,8 +775,7 @@ scphd_status scphd_merge_components(const double* comps, const uint8_t* flags, i
         uint8_t* d_flags = nullptr;
         int* d_n = nullptr;
         int* d_mem = nullptr;
-        const size_t cap = (size_t)n + 1, nchunk = (cap + 31) / 32;
-        size_t smem = 2 * cap * (sizeof(T) + 8) + 6 * cap * sizeof(T) + 3 * cap * 4 + 4 * nchunk * 4 + 2 * cap + 64;
+        size_t smem = merge_smem_bytes<T>(n + 1, 0, 4);
         T* d_sparse = nullptr;
         scphd_status st = SCPHD_OK;
         std::vector<T> out((size_t)n * kRow);
@@ -899,8 +897,7 @@ scphd_status merge_static_impl(unsigned char* base, const double* comps, const u
     CUDA_TRY(cudaMemset(d_mem, 0xff, sizeof(int) * (size_t)n));
     k_rows_from28<T><<<(n * kRow + 255) / 256, 256>>>(d_in, n, d_rows);
     g_launches.fetch_add(1, std::memory_order_relaxed);
-    const size_t cap = (size_t)n + 1, nchunk = (cap + 31) / 32;
-    const size_t smem = 2 * cap * (sizeof(T) + 8) + 6 * cap * sizeof(T) + 3 * cap * 4 + 4 * nchunk * 4 + 2 * cap + 64;
+    const size_t smem = merge_smem_bytes<T>(n + 1, 0, 4);
     CUDA_TRY(cudaFuncSetAttribute(k_merge_list<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_merge_list<T><<<1, 128, smem>>>(d_rows, d_flags, n, (T)min_separation, d_sparse, d_out, d_cnt, d_mem);
     g_launches.fetch_add(1, std::memory_order_relaxed);

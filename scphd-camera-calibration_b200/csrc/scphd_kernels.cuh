@@ -138,6 +138,7 @@ __global__ void __launch_bounds__(256) k_cloud_fit(Params prm, Bufs<T> b, int cu
     const int P = prm.P, Ps = prm.Ps;
     const T invP = T(1) / T(P);
     __shared__ int s_rd, s_wr;
+    __shared__ T s_km[8 * 72];   // per warp: P[21], S^-1[6], K[18], P'[21]
     if (threadIdx.x == 0) { s_rd = 0; s_wr = 0; }
     __syncthreads();
     for (int j = warp; j < G; j += blockDim.x >> 5) {
@@ -158,9 +159,10 @@ __global__ void __launch_bounds__(256) k_cloud_fit(Params prm, Bufs<T> b, int cu
                     uint32_t w0[4], w1[4];
                     philox((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 0), prm.key0, prm.key1, w0);
                     philox((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 1), prm.key0, prm.key1, w1);
-                    T z[8];
-                    Normals<T>::four(w0, z);
-                    Normals<T>::four(w1, z + 4);
+                    T z[6];
+                    Pair<T>::two(w0[0], w0[1], z[0], z[1]);
+                    Pair<T>::two(w0[2], w0[3], z[2], z[3]);
+                    Pair<T>::two(w1[0], w1[1], z[4], z[5]);
                     T y[6];
 #pragma unroll
                     for (int a = 0; a < 6; ++a) {
@@ -203,7 +205,8 @@ __global__ void __launch_bounds__(256) k_cloud_fit(Params prm, Bufs<T> b, int cu
                     uint32_t w[4];
                     philox((uint32_t)s, (uint32_t)j, (uint32_t)p, ctr_word3(pred_frame, ST_FEAT, 0), prm.key0, prm.key1, w);
                     T z[4];
-                    Normals<T>::four(w, z);
+                    Pair<T>::two(w[0], w[1], z[0], z[1]);
+                    Pair<T>::two(w[2], w[3], z[2], z[3]);
 #pragma unroll
                     for (int q = 0; q < 3; ++q) {
                         T a = (T)prm.feat_std[q] * z[q];
@@ -270,26 +273,19 @@ __global__ void __launch_bounds__(256) k_cloud_fit(Params prm, Bufs<T> b, int cu
 #pragma unroll
         for (int i = 0; i < 21; ++i) cv[i] = warp_sum(cv[i]) * covscale;
         const T pbar = (T)((double)n_in * m.pd / (double)P);
+        // fitted row: lane q writes element q (W, pD, mean[6], packed cov[21])
         T* fr = b.fit + ((size_t)p * prm.Gcap + j) * kRow;
-        if (lane == 0) {
-            fr[0] = W;
-            fr[1] = pbar;
+        {
+            T v = W;
+            if (lane == 1) v = pbar;
 #pragma unroll
-            for (int a = 0; a < 6; ++a) fr[2 + a] = mu[a];
+            for (int a = 0; a < 6; ++a) if (lane == 2 + a) v = mu[a];
 #pragma unroll
-            for (int i = 0; i < 21; ++i) fr[8 + i] = cv[i];
+            for (int i = 0; i < 21; ++i) if (lane == 8 + i) v = cv[i];
+            if (lane < 29) fr[lane] = v;
         }
-        __syncwarp();
-        if (lane == 0) {
-            T rowbuf[kRow];
-            rowbuf[0] = W; rowbuf[1] = pbar;
-            for (int a = 0; a < 6; ++a) rowbuf[2 + a] = mu[a];
-            for (int i = 0; i < 21; ++i) rowbuf[8 + i] = cv[i];
-            T pr[kPrep];
-            kalman_prep<T, K>(rowbuf, m, pr);
-            T* dst = b.prep + ((size_t)p * prm.Gcap + j) * kPrep;
-            for (int i = 0; i < kPrep - 1; ++i) dst[i] = pr[i];
-        }
+        warp_kalman_prep<T, K>(W, pbar, cv, m, s_km + warp * 72, lane,
+                               b.prep + ((size_t)p * prm.Gcap + j) * kPrep);
         // retained non-detection cloud: predicted world samples, weights 1 - pD
         const T wnd = W * (T(1) - pbar);
         if (wnd >= (T)prm.min_weight) {
@@ -560,25 +556,139 @@ __device__ __forceinline__ void uf_unite(int* uf, int a, int b) {
     }
 }
 
+// Shared-memory working set of the merge (per CTA); sizes are derived from the
+// survivor capacity S and map capacity G by merge_smem_bytes().
 template <typename T> struct MergeScratch {
-    T* pf;          // n x 6: mean[0..3), cov diagonal [0..3) (prefilter data)
-    uint8_t* flag;  // n: merged
-    uint8_t* is_center;   // n
-    int* uf;        // n: union-find parent, then component label (= smallest index)
-    int* roots;     // n
+    float* pf;            // S x 6: mean[0..3), cov diagonal [0..3) (prefilter data)
+    uint8_t* flag;        // S: merged
+    uint8_t* is_center;   // S
+    int* lab;             // S: union-find parent, then the component's root
+    int* cidx;            // S: component index of a root; later the queue of large components
+    int* start;           // S + 1: member range of each component in perm
+    int* fill;            // S
+    int* perm;            // cap: survivors grouped by component (first: survivors in u order)
     uint32_t* masks;      // (blockDim/32) x nchunk member masks
     int nchunk;
 };
 
+constexpr int kSmallComp = 8;   // components up to this size are merged by one thread
+
+__host__ __device__ inline int next_pow2(int x) {
+    int p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+// sort capacity (survivors, then map entries), in elements
+__host__ __device__ inline int merge_sort_cap(int S, int G) {
+    int a = next_pow2(S), b = S + G;
+    return a > b ? a : b;
+}
+
+template <typename T> inline size_t merge_smem_bytes(int S, int G, int nwarps) {
+    const size_t cap = merge_sort_cap(S, G), nchunk = (S + 31) / 32;
+    return cap * (sizeof(T) + 8) + 6 * (size_t)S * sizeof(float) + 3 * (size_t)S * 4 + cap * 4 +
+           (size_t)(S + 1) * 4 + (size_t)(S + G) * 4 + (size_t)nwarps * nchunk * 4 + 2 * (size_t)S + 64;
+}
+
 template <typename T>
-__device__ __forceinline__ bool could_merge(const T* a, const T* b, T min_sep, T margin) {
+__device__ inline void carve_merge_smem(unsigned char* smem, int S, int G, T*& s_w, uint32_t*& s_key, int*& s_r,
+                                        int*& s_pos, MergeScratch<T>& ms) {
+    const int cap = merge_sort_cap(S, G);
+    s_w = reinterpret_cast<T*>(smem);
+    s_key = reinterpret_cast<uint32_t*>(s_w + cap);
+    s_r = reinterpret_cast<int*>(s_key + cap);
+    ms.pf = reinterpret_cast<float*>(s_r + cap);
+    ms.lab = reinterpret_cast<int*>(ms.pf + 6 * S);
+    ms.cidx = ms.lab + S;
+    ms.fill = ms.cidx + S;
+    ms.perm = ms.fill + S;
+    ms.start = ms.perm + cap;
+    s_pos = ms.start + S + 1;
+    ms.nchunk = (S + 31) / 32;
+    ms.masks = reinterpret_cast<uint32_t*>(s_pos + S + G);
+    ms.flag = reinterpret_cast<uint8_t*>(ms.masks + (blockDim.x / 32) * ms.nchunk);
+    ms.is_center = ms.flag + S;
+}
+
+__device__ __forceinline__ bool could_merge_f(const float* a, const float* b, float min_sep, float margin) {
     bool ok = true;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        T d = a[k] - b[k];
+        float d = a[k] - b[k];
         ok = ok && (d * d <= min_sep * (a[3 + k] + b[3 + k]) * margin);
     }
     return ok;
+}
+
+// Moment-matched merge of the members (ascending survivor indices mem[k] for the set
+// bits k of mbits) into centre c, written to sparse[c]; reference order of the sums
+// (kernels.cu:770-843): weights and weighted means, then covariances about the mean.
+template <typename T, typename Src>
+__device__ void merge_members_thread(const Src& src, const T* s_w, const int* s_r, const int* mem, uint32_t mbits,
+                                     int c, const T* cmu, const T* ccov, T* sparse) {
+    T W = 0, acc[6] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t mb = mbits; mb; mb &= mb - 1) {
+        int i = mem[__ffs(mb) - 1];
+        T w = s_w[i], mu[6];
+        src.mean(s_r[i], mu);
+        W += w;
+#pragma unroll
+        for (int a = 0; a < 6; ++a) acc[a] += w * mu[a];
+    }
+    T row[28];
+    row[0] = W;
+#pragma unroll
+    for (int a = 0; a < 6; ++a) row[1 + a] = acc[a] / W;
+    T cv[21];
+#pragma unroll
+    for (int e = 0; e < 21; ++e) cv[e] = 0;
+    for (uint32_t mb = mbits; mb; mb &= mb - 1) {
+        int i = mem[__ffs(mb) - 1];
+        T w = s_w[i], mu[6], d[6];
+        src.mean(s_r[i], mu);
+        const T* sc = src.cov(s_r[i]);
+#pragma unroll
+        for (int a = 0; a < 6; ++a) d[a] = row[1 + a] - mu[a];
+#pragma unroll
+        for (int a = 0; a < 6; ++a)
+#pragma unroll
+            for (int bb = 0; bb <= a; ++bb) cv[tri(a, bb)] += w * (sc[tri(a, bb)] + d[a] * d[bb]);
+    }
+#pragma unroll
+    for (int e = 0; e < 21; ++e) row[7 + e] = cv[e] / W;
+    T L[21];
+    const bool pd = chol6(row + 7, L);
+    T* o = sparse + (size_t)c * kRow;
+    if (pd) {
+#pragma unroll
+        for (int q = 0; q < 28; ++q) o[q] = row[q];
+    } else {   // "bad hack, just keep the max feature" (kernels.cu:855-862)
+        o[0] = s_w[c];
+#pragma unroll
+        for (int a = 0; a < 6; ++a) o[1 + a] = cmu[a];
+#pragma unroll
+        for (int e = 0; e < 21; ++e) o[7 + e] = ccov[e];
+    }
+}
+
+// In-place bitonic sort of (key, payload) ascending by key over n_pad (power of 2) slots.
+__device__ void sort_keys(uint32_t* key, int* val, int n_pad) {
+    for (int k = 2; k <= n_pad; k <<= 1) {
+        for (int jj = k >> 1; jj > 0; jj >>= 1) {
+            for (int i = threadIdx.x; i < n_pad; i += blockDim.x) {
+                int ixj = i ^ jj;
+                if (ixj > i) {
+                    bool up = (i & k) == 0;
+                    if ((key[i] > key[ixj]) == up) {
+                        uint32_t tk = key[i]; key[i] = key[ixj]; key[ixj] = tk;
+                        int tv = val[i]; val[i] = val[ixj]; val[ixj] = tv;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
 }
 
 // Greedy reduction of phdUpdateMergeKernel (src/kernels.cu:693-866) over n
@@ -588,101 +698,210 @@ __device__ __forceinline__ bool could_merge(const T* a, const T* b, T min_sep, T
 // is kept if PD, else the centre.  Since x' A^-1 x >= x_k^2 / A_kk for SPD A, two
 // survivors failing the diagonal bound on u, v or d (with a safety margin) can
 // never merge; the greedy sequence therefore decomposes exactly over the connected
-// components of the "may merge" graph, and each warp runs the greedy loop on whole
-// components independently.  Merged rows are written to sparse[centre index];
-// returns the index of the first centre that absorbed nothing (the reference's
-// loop ends there), or n.  Block-wide call.
+// components of the "may merge" graph.  Components are listed with their members in
+// sorted order; one thread runs the greedy loop of a small component, one warp that
+// of a large one.  Merged rows are written to sparse[centre index]; returns the
+// index of the first centre that absorbed nothing (the reference's loop ends there),
+// or n.  Block-wide call.
 template <typename T, typename Src>
 __device__ int merge_components(const Src& src, const T* s_w, const int* s_r, int n, MergeScratch<T> ms,
-                                T min_sep, T margin, T* sparse, int* member_out, unsigned long long* counters) {
-    __shared__ int s_nroots, s_take, s_stop, s_evals, s_ncent;
+                                uint32_t* ukey, T min_sep, T* sparse, int* member_out,
+                                unsigned long long* counters) {
+    __shared__ int s_ncomp, s_take, s_nlarge, s_take_large, s_stop, s_evals;
+    __shared__ int s_tmp[40];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const float fsep = (float)min_sep, fmargin = 1.01f;
     for (int i = tid; i < n; i += blockDim.x) {
         T mu[6];
         src.mean(s_r[i], mu);
         const T* cv = src.cov(s_r[i]);
-        ms.pf[i * 6 + 0] = mu[0]; ms.pf[i * 6 + 1] = mu[1]; ms.pf[i * 6 + 2] = mu[2];
-        ms.pf[i * 6 + 3] = cv[0]; ms.pf[i * 6 + 4] = cv[2]; ms.pf[i * 6 + 5] = cv[5];
+        float* pf = ms.pf + i * 6;
+        pf[0] = (float)mu[0]; pf[1] = (float)mu[1]; pf[2] = (float)mu[2];
+        pf[3] = (float)cv[0]; pf[4] = (float)cv[2]; pf[5] = (float)cv[5];
         ms.flag[i] = 0;
         ms.is_center[i] = 0;
-        ms.uf[i] = i;
+        ms.lab[i] = i;
     }
-    if (tid == 0) { s_nroots = 0; s_take = 0; s_stop = n; s_evals = 0; s_ncent = 0; }
+    if (tid == 0) { s_ncomp = 0; s_take = 0; s_nlarge = 0; s_take_large = 0; s_stop = n; s_evals = 0; }
     __syncthreads();
-    // "may merge" edges -> components
-    for (int i = tid; i < n; i += blockDim.x) {
-        const T* a = ms.pf + i * 6;
-        for (int j = i + 1; j < n; ++j)
-            if (could_merge(a, ms.pf + j * 6, min_sep, margin)) uf_unite(ms.uf, i, j);
-    }
-    __syncthreads();
-    for (int i = tid; i < n; i += blockDim.x) {
-        int r = uf_find(ms.uf, i);
-        if (r == i) ms.roots[atomicAdd(&s_nroots, 1)] = i;
-    }
-    __syncthreads();
-    for (int i = tid; i < n; i += blockDim.x) ms.uf[i] = uf_find(ms.uf, i);
-    __syncthreads();
-    uint32_t* masks = ms.masks + (size_t)warp * ms.nchunk;
-    const int nch = (n + 31) >> 5;   // <= ms.nchunk
-    int evals = 0;
-    while (true) {
-        int comp = 0;
-        if (lane == 0) comp = atomicAdd(&s_take, 1);
-        comp = __shfl_sync(0xffffffffu, comp, 0);
-        if (comp >= s_nroots) break;
-        const int r = ms.roots[comp];
-        int next = r;
-        while (true) {
-            // centre: first unmerged member of the component
-            int c = -1;
-            for (int base = next & ~31; base < n; base += 32) {
-                int i = base + lane;
-                bool pred = i >= next && i < n && ms.uf[i] == r && !ms.flag[i];
-                unsigned bal = __ballot_sync(0xffffffffu, pred);
-                if (bal) { c = base + __ffs(bal) - 1; break; }
-            }
-            if (c < 0) break;
-            next = c + 1;
-            T cmu[6], ccov[21];
-            src.mean(s_r[c], cmu);
-            const T* cc = src.cov(s_r[c]);
+    // "may merge" edges -> union-find.  |du| <= sqrt(sep*margin*(Suu_i + max Suu)) is
+    // necessary for the bound on u, so with the survivors in u order each one scans
+    // forward only over that window.
+    __shared__ float s_maxsuu;
+    {
+        float mx = 0.f;
+        for (int i = tid; i < n; i += blockDim.x) {
+            mx = fmaxf(mx, ms.pf[i * 6 + 3]);
+            const float u = ms.pf[i * 6 + 0];
+            uint32_t bits = __float_as_uint(u);
+            ukey[i] = (bits & 0x80000000u) ? ~bits : (bits | 0x80000000u);   // orderable float key
+            ms.perm[i] = i;
+        }
 #pragma unroll
-            for (int q = 0; q < 21; ++q) ccov[q] = cc[q];
-            // members: unmerged survivors of the component within distance
-            const int c0 = c >> 5;
+        for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (tid == 0) s_maxsuu = 0.f;
+        __syncthreads();
+        if (lane == 0) atomicMax(reinterpret_cast<int*>(&s_maxsuu), __float_as_int(mx));   // mx >= 0
+        const int np2 = next_pow2(n);
+        for (int i = n + tid; i < np2; i += blockDim.x) { ukey[i] = 0xffffffffu; ms.perm[i] = 0x7fffffff; }
+        __syncthreads();
+        sort_keys(ukey, ms.perm, np2);
+    }
+    const float maxsuu = s_maxsuu;
+    for (int q = tid; q < n; q += blockDim.x) {
+        const int i = ms.perm[q];
+        float a[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) a[k] = ms.pf[i * 6 + k];
+        const float reach = sqrtf(fsep * fmargin * (a[3] + maxsuu)) * 1.0001f;
+        for (int q2 = q + 1; q2 < n; ++q2) {
+            const int j = ms.perm[q2];
+            const float* bj = ms.pf + j * 6;
+            if (bj[0] - a[0] > reach) break;
+            if (could_merge_f(a, bj, fsep, fmargin)) uf_unite(ms.lab, i, j);
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += blockDim.x) {
+        if (uf_find(ms.lab, i) == i) {
+            int c = atomicAdd(&s_ncomp, 1);
+            ms.cidx[i] = c;
+            ms.start[c] = 0;
+            ms.fill[c] = 0;
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += blockDim.x) ms.lab[i] = uf_find(ms.lab, i);
+    __syncthreads();
+    const int ncomp = s_ncomp;
+    for (int i = tid; i < n; i += blockDim.x) atomicAdd(&ms.start[ms.cidx[ms.lab[i]]], 1);
+    __syncthreads();
+    block_exclusive_scan(ms.start, ncomp, s_tmp);
+    if (tid == 0) ms.start[ncomp] = n;
+    __syncthreads();
+    // members of each component in ascending order (chunks in order, ranks by lane)
+    if (warp == 0) {
+        for (int base = 0; base < n; base += 32) {
+            const int i = base + lane;
+            const bool valid = i < n;
+            const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+            if (valid) {
+                const int c = ms.cidx[ms.lab[i]];
+                const unsigned grp = __match_any_sync(vmask, c);
+                const int leader = __ffs(grp) - 1;
+                const int rank = __popc(grp & ((1u << lane) - 1u));
+                int off = 0;
+                if (lane == leader) {
+                    off = ms.fill[c];
+                    ms.fill[c] = off + __popc(grp);
+                }
+                off = __shfl_sync(grp, off, leader);
+                ms.perm[ms.start[c] + off + rank] = i;
+            }
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    int evals = 0;
+    // small components: one thread each; large ones are queued for the warps
+    while (true) {
+        const int c = atomicAdd(&s_take, 1);
+        if (c >= ncomp) break;
+        const int s0 = ms.start[c], cnt = ms.start[c + 1] - s0;
+        if (cnt > kSmallComp) {
+            ms.cidx[atomicAdd(&s_nlarge, 1)] = c;   // roots' indices are no longer needed
+            continue;
+        }
+        const int* mem = ms.perm + s0;
+        uint32_t done = 0;
+        while (true) {
+            const int k0 = __ffs(~done) - 1;
+            if (k0 < 0 || k0 >= cnt) break;
+            const int cc = mem[k0];
+            T cmu[6], ccov[21];
+            src.mean(s_r[cc], cmu);
+            const T* cp = src.cov(s_r[cc]);
+#pragma unroll
+            for (int q = 0; q < 21; ++q) ccov[q] = cp[q];
+            uint32_t mbits = 0;
+            for (int k = k0; k < cnt; ++k) {
+                if ((done >> k) & 1u) continue;
+                const int i = mem[k];
+                if (!could_merge_f(ms.pf + cc * 6, ms.pf + i * 6, fsep, fmargin)) continue;
+                ++evals;
+                T mu[6];
+                src.mean(s_r[i], mu);
+                if (mahal6(cmu, ccov, mu, src.cov(s_r[i])) < min_sep) mbits |= 1u << k;
+            }
+            if (!mbits) {   // merged weight 0: the reference's loop ends (kernels.cu:783-784)
+                atomicMin(&s_stop, cc);
+                break;
+            }
+            merge_members_thread(src, s_w, s_r, mem, mbits, cc, cmu, ccov, sparse);
+            ms.is_center[cc] = 1;
+            if (member_out)
+                for (uint32_t mb = mbits; mb; mb &= mb - 1) member_out[s_r[mem[__ffs(mb) - 1]]] = cc;
+            done |= mbits;
+        }
+    }
+    __syncthreads();
+    // large components: one warp each, lanes over the member range
+    uint32_t* masks = ms.masks + (size_t)warp * ms.nchunk;
+    while (true) {
+        int q = 0;
+        if (lane == 0) q = atomicAdd(&s_take_large, 1);
+        q = __shfl_sync(0xffffffffu, q, 0);
+        if (q >= s_nlarge) break;
+        const int c = ms.cidx[q];
+        const int s0 = ms.start[c], cnt = ms.start[c + 1] - s0;
+        const int* mem = ms.perm + s0;
+        const int nch = (cnt + 31) >> 5;
+        int next = 0;
+        while (true) {
+            int k0 = -1;
+            for (int ch = next >> 5; ch < nch; ++ch) {
+                const int k = ch * 32 + lane;
+                const bool pred = k >= next && k < cnt && !ms.flag[mem[k]];
+                const unsigned bal = __ballot_sync(0xffffffffu, pred);
+                if (bal) { k0 = ch * 32 + __ffs(bal) - 1; break; }
+            }
+            if (k0 < 0) break;
+            next = k0 + 1;
+            const int cc = mem[k0];
+            T cmu[6], ccov[21];
+            src.mean(s_r[cc], cmu);
+            const T* cp = src.cov(s_r[cc]);
+#pragma unroll
+            for (int qq = 0; qq < 21; ++qq) ccov[qq] = cp[qq];
             bool any = false;
-            for (int ch = c0; ch < nch; ++ch) {
-                int i = ch * 32 + lane;
-                bool mem = false;
-                if (i >= c && i < n && ms.uf[i] == r && !ms.flag[i]) {
-                    T pfc[6] = {cmu[0], cmu[1], cmu[2], ccov[0], ccov[2], ccov[5]};
-                    if (could_merge(pfc, ms.pf + i * 6, min_sep, margin)) {
+            for (int ch = k0 >> 5; ch < nch; ++ch) {
+                const int k = ch * 32 + lane;
+                bool m = false;
+                if (k >= k0 && k < cnt) {
+                    const int i = mem[k];
+                    if (!ms.flag[i] && could_merge_f(ms.pf + cc * 6, ms.pf + i * 6, fsep, fmargin)) {
                         ++evals;
                         T mu[6];
                         src.mean(s_r[i], mu);
-                        mem = mahal6(cmu, ccov, mu, src.cov(s_r[i])) < min_sep;
+                        m = mahal6(cmu, ccov, mu, src.cov(s_r[i])) < min_sep;
                     }
                 }
-                unsigned bal = __ballot_sync(0xffffffffu, mem);
+                const unsigned bal = __ballot_sync(0xffffffffu, m);
                 if (lane == 0) masks[ch] = bal;
                 any = any || bal;
             }
             __syncwarp();
-            if (!any) {   // merged weight 0: the reference's loop ends (kernels.cu:783-784)
-                if (lane == 0) atomicMin(&s_stop, c);
+            if (!any) {
+                if (lane == 0) atomicMin(&s_stop, cc);
                 break;
             }
-            // weight and mean, members in index order; lane a < 6 owns mean[a]
+            // weight and mean (lane a < 6 owns mean[a]), members in ascending order
             T accw = 0, accm = 0;
-            for (int ch = c0; ch < nch; ++ch) {
-                unsigned mk = masks[ch];
-                while (mk) {
-                    int ii = ch * 32 + __ffs(mk) - 1;
-                    mk &= mk - 1;
-                    T w = s_w[ii];
-                    T mu[6];
-                    src.mean(s_r[ii], mu);
+            for (int ch = k0 >> 5; ch < nch; ++ch) {
+                for (unsigned mk = masks[ch]; mk; mk &= mk - 1) {
+                    const int i = mem[ch * 32 + __ffs(mk) - 1];
+                    T w = s_w[i], mu[6];
+                    src.mean(s_r[i], mu);
                     accw += w;
                     T sel = mu[0];
 #pragma unroll
@@ -691,32 +910,29 @@ __device__ int merge_components(const Src& src, const T* s_w, const int* s_r, in
                 }
             }
             const T W = accw;
-            T mean[6];
             const T my_mean = (lane < 6) ? accm / W : T(0);
+            T mean[6];
 #pragma unroll
             for (int a = 0; a < 6; ++a) mean[a] = __shfl_sync(0xffffffffu, my_mean, a);
-            // covariance: lane e < 21 owns packed entry e = (ea, eb)
             int ea = 0;
             while ((ea + 1) * (ea + 2) / 2 <= lane && ea < 5) ++ea;
             const int eb = lane - ea * (ea + 1) / 2;
             T accc = 0;
-            for (int ch = c0; ch < nch; ++ch) {
-                unsigned mk = masks[ch];
-                int i = ch * 32 + lane;
-                if (mk & (1u << lane)) {
+            for (int ch = k0 >> 5; ch < nch; ++ch) {
+                const unsigned mk0 = masks[ch];
+                const int k = ch * 32 + lane;
+                if (mk0 & (1u << lane)) {
+                    const int i = mem[k];
                     ms.flag[i] = 1;
-                    if (member_out) member_out[s_r[i]] = c;
+                    if (member_out) member_out[s_r[i]] = cc;
                 }
-                while (mk) {
-                    int ii = ch * 32 + __ffs(mk) - 1;
-                    mk &= mk - 1;
+                for (unsigned mk = mk0; mk; mk &= mk - 1) {
+                    const int i = mem[ch * 32 + __ffs(mk) - 1];
                     if (lane < 21) {
-                        T w = s_w[ii];
-                        T mu[6];
-                        src.mean(s_r[ii], mu);
-                        const T* cv = src.cov(s_r[ii]);
-                        T da = mean[ea] - mu[ea], db = mean[eb] - mu[eb];
-                        accc += w * (cv[lane] + da * db);
+                        T w = s_w[i], mu[6];
+                        src.mean(s_r[i], mu);
+                        const T* cv = src.cov(s_r[i]);
+                        accc += w * (cv[lane] + (mean[ea] - mu[ea]) * (mean[eb] - mu[eb]));
                     }
                 }
             }
@@ -726,20 +942,18 @@ __device__ int merge_components(const Src& src, const T* s_w, const int* s_r, in
 #pragma unroll
             for (int a = 0; a < 6; ++a) row[1 + a] = mean[a];
 #pragma unroll
-            for (int q = 0; q < 21; ++q) row[7 + q] = __shfl_sync(0xffffffffu, my_cov, q);
+            for (int qq = 0; qq < 21; ++qq) row[7 + qq] = __shfl_sync(0xffffffffu, my_cov, qq);
             T L[21];
             const bool pd = chol6(row + 7, L);
-            T* o = sparse + (size_t)c * kRow;
+            T* o = sparse + (size_t)cc * kRow;
             if (lane < 28) {
-                T v;
-                if (pd) v = row[0];
-                else v = s_w[c];   // "bad hack, just keep the max feature" (kernels.cu:855-862)
+                T v = pd ? row[0] : s_w[cc];
 #pragma unroll
-                for (int q = 1; q < 28; ++q)
-                    if (lane == q) v = pd ? row[q] : (q < 7 ? cmu[q - 1] : ccov[q - 7]);
+                for (int qq = 1; qq < 28; ++qq)
+                    if (lane == qq) v = pd ? row[qq] : (qq < 7 ? cmu[qq - 1] : ccov[qq - 7]);
                 o[lane] = v;
             }
-            if (lane == 0) ms.is_center[c] = 1;
+            if (lane == 0) ms.is_center[cc] = 1;
             __syncwarp();
         }
     }
@@ -755,21 +969,15 @@ __global__ void __launch_bounds__(128) k_merge(Params prm, Bufs<T> b, int cur, i
     const int p = blockIdx.x;
     const int tid = threadIdx.x;
     const int G = b.map_n[cur][b.src[p]];
-    const int n = min(b.surv_n[p], prm.Scap);
-    const int S2 = 2 * prm.Scap + 2 * prm.Gcap;   // sort capacity (survivors, then map entries)
-    int n_pad = 1;
-    while (n_pad < n) n_pad <<= 1;
-    T* s_w = reinterpret_cast<T*>(smem);
-    uint32_t* s_key = reinterpret_cast<uint32_t*>(s_w + S2);
-    int* s_r = reinterpret_cast<int*>(s_key + S2);
-    T* s_pf = reinterpret_cast<T*>(s_r + S2);
-    int* s_uf = reinterpret_cast<int*>(s_pf + 6 * prm.Scap);
-    int* s_roots = s_uf + prm.Scap;
-    int* s_pos = s_roots + prm.Scap;                              // Scap + Gcap
-    uint32_t* s_masks = reinterpret_cast<uint32_t*>(s_pos + prm.Scap + prm.Gcap);
-    const int nchunk = (prm.Scap + 31) / 32;
-    uint8_t* s_flag = reinterpret_cast<uint8_t*>(s_masks + (blockDim.x / 32) * nchunk);
-    uint8_t* s_cent = s_flag + prm.Scap;
+    const int n_all_surv = b.surv_n[p];
+    const int n = min(n_all_surv, prm.Scap);
+    const int n_pad = next_pow2(n);
+    T* s_w;
+    uint32_t* s_key;
+    int* s_r;
+    int* s_pos;
+    MergeScratch<T> ms;
+    carve_merge_smem<T>(smem, prm.Scap, prm.Gcap, s_w, s_key, s_r, s_pos, ms);
     __shared__ int s_tmp[40];
     for (int i = tid; i < n_pad; i += blockDim.x) {
         if (i < n) {
@@ -809,17 +1017,14 @@ __global__ void __launch_bounds__(128) k_merge(Params prm, Bufs<T> b, int cur, i
     src.bcov[tri(4, 4)] = (T)prm.var_vv0;
     src.bcov[tri(5, 5)] = (T)prm.var_vd0;
     T* sparse = b.mtmp + (size_t)p * prm.Scap * kRow;
-    const T margin = sizeof(T) == 4 ? T(1.05) : T(1.000001);
-    MergeScratch<T> ms{s_pf, s_flag, s_cent, s_uf, s_roots, s_masks, nchunk};
-    const int stop = merge_components<T>(src, s_w, s_r, n, ms, (T)prm.min_sep, margin, sparse, nullptr,
-                                         b.counters);
+    const int stop = merge_components<T>(src, s_w, s_r, n, ms, s_key, (T)prm.min_sep, sparse, nullptr, b.counters);
     // merged list in centre order (centres after a stop are dropped, as the reference's loop ends there)
-    for (int i = tid; i < n; i += blockDim.x) s_pos[i] = (i < stop && s_cent[i]) ? 1 : 0;
+    for (int i = tid; i < n; i += blockDim.x) s_pos[i] = (i < stop && ms.is_center[i]) ? 1 : 0;
     __syncthreads();
     const int n_out = block_exclusive_scan(s_pos, n, s_tmp);
     T* out = b.merged + (size_t)p * prm.Scap * kRow;
     for (int i = tid; i < n; i += blockDim.x) {
-        if (i < stop && s_cent[i]) {
+        if (i < stop && ms.is_center[i]) {
             const T* sr = sparse + (size_t)i * kRow;
             T* dr = out + (size_t)s_pos[i] * kRow;
             for (int q = 0; q < 28; ++q) dr[q] = sr[q];
@@ -830,6 +1035,7 @@ __global__ void __launch_bounds__(128) k_merge(Params prm, Bufs<T> b, int cur, i
     // entries e < n_out are merged, e >= n_out are the Gaussians j = e - n_out
     const T minw = (T)prm.min_weight;
     const int n_all = n_out + G;
+    int n_valid_part = 0;
     for (int e = tid; e < n_all; e += blockDim.x) {
         T w;
         if (e < n_out) {
@@ -840,30 +1046,30 @@ __global__ void __launch_bounds__(128) k_merge(Params prm, Bufs<T> b, int cur, i
             w = (wnd >= minw) ? wnd : T(-1);   // -1: not retained
         }
         s_w[e] = w;
-        s_pos[e] = w >= T(0) ? 1 : 0;
+        n_valid_part += w >= T(0);
+    }
+    __shared__ int s_nvalid;
+    if (tid == 0) s_nvalid = 0;
+    __syncthreads();
+    atomicAdd(&s_nvalid, n_valid_part);
+    __syncthreads();
+    const bool cut = s_nvalid > prm.Gcap;
+    // keep: retained, and when over capacity among the Gcap largest (ties by entry order)
+    for (int e = tid; e < n_all; e += blockDim.x) {
+        const T w = s_w[e];
+        int keep = w >= T(0);
+        if (keep && cut) {
+            int rank = 0;
+            for (int f = 0; f < n_all; ++f) {
+                const T v = s_w[f];
+                rank += (v > w) || (v == w && f < e);
+            }
+            keep = rank < prm.Gcap;
+        }
+        s_pos[e] = keep;
     }
     __syncthreads();
-    int total = block_exclusive_scan(s_pos, n_all, s_tmp);
-    if (total > prm.Gcap) {
-        // keep the Gcap largest weights (ties in entry order): sort copies of the weights
-        int np2 = 1;
-        while (np2 < n_all) np2 <<= 1;
-        for (int e = tid; e < np2; e += blockDim.x) {
-            s_key[e] = (uint32_t)e;
-            s_r[e] = e;
-            if (e >= n_all) s_w[e] = T(-2);
-        }
-        __syncthreads();
-        sort_survivors(s_w, s_key, s_r, np2);   // descending weight, then entry order
-        for (int e = tid; e < n_all; e += blockDim.x) s_pos[e] = 0;
-        __syncthreads();
-        for (int e = tid; e < prm.Gcap; e += blockDim.x)
-            if (s_w[e] >= T(0)) s_pos[s_r[e]] = 1;
-        __syncthreads();
-        if (tid == 0) atomicAdd(&b.counters[0], 1ull);
-        total = block_exclusive_scan(s_pos, n_all, s_tmp);
-    }
-    // write the kept entries in entry order
+    const int total = block_exclusive_scan(s_pos, n_all, s_tmp);
     const int wrow = p;   // the new map lives at row p of the other buffer
     T* mo = b.map[cur ^ 1] + (size_t)wrow * prm.Gcap * kRow;
     int* mr = b.map_ref[cur ^ 1] + (size_t)wrow * prm.Gcap;
@@ -877,8 +1083,7 @@ __global__ void __launch_bounds__(128) k_merge(Params prm, Bufs<T> b, int cur, i
             mr[pos] = -1 - e;
         } else {
             const int j = e - n_out;
-            const T* fr = b.fit + ((size_t)p * prm.Gcap + j) * kRow;
-            mo[(size_t)pos * kRow] = fr[0] * (T(1) - fr[1]);
+            mo[(size_t)pos * kRow] = s_w[e];
             mr[pos] = p * prm.Gcap + j;
         }
     }
@@ -887,9 +1092,11 @@ __global__ void __launch_bounds__(128) k_merge(Params prm, Bufs<T> b, int cur, i
         b.map_n[cur ^ 1][wrow] = total;
         double* me = b.map_ext[cur ^ 1] + 12 * wrow;
         for (int q = 0; q < 12; ++q) me[q] = fixed ? 0.0 : b.ext[12 * p + q];
+        if (cut) atomicAdd(&b.counters[0], 1ull);
         atomicAdd(&b.counters[5], (unsigned long long)n);
         atomicAdd(&b.counters[7], (unsigned long long)n);
         atomicAdd(&b.counters[11], (unsigned long long)n_out);
+        atomicMax(&b.counters[13], (unsigned long long)n_all_surv);
     }
 }
 
@@ -1074,9 +1281,10 @@ __global__ void __launch_bounds__(256) k_materialize(Params prm, Bufs<T> b, int 
                 const uint32_t key_i = (uint32_t)(-1 - ref);
                 philox((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 0), prm.key0, prm.key1, w0);
                 philox((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 1), prm.key0, prm.key1, w1);
-                T z[8];
-                Normals<T>::four(w0, z);
-                Normals<T>::four(w1, z + 4);
+                T z[6];
+                Pair<T>::two(w0[0], w0[1], z[0], z[1]);
+                Pair<T>::two(w0[2], w0[3], z[2], z[3]);
+                Pair<T>::two(w1[0], w1[1], z[4], z[5]);
                 T y[6];
                 for (int a = 0; a < 6; ++a) {
                     T v = 0;
@@ -1094,7 +1302,8 @@ __global__ void __launch_bounds__(256) k_materialize(Params prm, Bufs<T> b, int 
                 uint32_t w[4];
                 philox((uint32_t)s, (uint32_t)j, (uint32_t)p, ctr_word3(pred_frame, ST_FEAT, 0), prm.key0, prm.key1, w);
                 T z[4];
-                Normals<T>::four(w, z);
+                Pair<T>::two(w[0], w[1], z[0], z[1]);
+                Pair<T>::two(w[2], w[3], z[2], z[3]);
                 const T dtT = (T)dt, half_dt2 = T(0.5) * (T)dt * (T)dt;
                 for (int q = 0; q < 3; ++q) {
                     T a = (T)prm.feat_std[q] * z[q];
@@ -1115,7 +1324,8 @@ __global__ void __launch_bounds__(256) k_materialize(Params prm, Bufs<T> b, int 
 }
 
 // ---------------------------------------------------------------- stand-alone merge
-// phdUpdateMergeKernel on an explicit component list (rows of kRow) with prune flags.
+// phdUpdateMergeKernel on an explicit component list (rows of kRow) with prune flags;
+// shared memory as merge_smem_bytes<T>(n_all + 1, 0, 4).
 template <typename T>
 __global__ void __launch_bounds__(128) k_merge_list(const T* rows, const uint8_t* flags_in, int n_all,
                                                     T min_sep, T* sparse, T* out, int* n_out_p, int* member_of) {
@@ -1128,20 +1338,13 @@ __global__ void __launch_bounds__(128) k_merge_list(const T* rows, const uint8_t
     }
     __syncthreads();
     const int n = s_n;
-    int n_pad = 1;
-    while (n_pad < n) n_pad <<= 1;
-    const int cap = n_all + 1;
-    T* s_w = reinterpret_cast<T*>(smem);
-    uint32_t* s_key = reinterpret_cast<uint32_t*>(s_w + 2 * cap);
-    int* s_r = reinterpret_cast<int*>(s_key + 2 * cap);
-    T* s_pf = reinterpret_cast<T*>(s_r + 2 * cap);
-    int* s_uf = reinterpret_cast<int*>(s_pf + 6 * cap);
-    int* s_roots = s_uf + cap;
-    int* s_pos = s_roots + cap;
-    const int nchunk = (cap + 31) / 32;
-    uint32_t* s_masks = reinterpret_cast<uint32_t*>(s_pos + cap);
-    uint8_t* s_flag = reinterpret_cast<uint8_t*>(s_masks + (blockDim.x / 32) * nchunk);
-    uint8_t* s_cent = s_flag + cap;
+    const int n_pad = next_pow2(n);
+    T* s_w;
+    uint32_t* s_key;
+    int* s_r;
+    int* s_pos;
+    MergeScratch<T> ms;
+    carve_merge_smem<T>(smem, n_all + 1, 0, s_w, s_key, s_r, s_pos, ms);
     if (threadIdx.x == 0) {
         int k = 0;
         for (int i = 0; i < n_all; ++i)
@@ -1156,14 +1359,12 @@ __global__ void __launch_bounds__(128) k_merge_list(const T* rows, const uint8_t
     __syncthreads();
     sort_survivors(s_w, s_key, s_r, n_pad);
     ListSource<T> src{rows};
-    const T margin = sizeof(T) == 4 ? T(1.05) : T(1.000001);
-    MergeScratch<T> ms{s_pf, s_flag, s_cent, s_uf, s_roots, s_masks, nchunk};
-    const int stop = merge_components<T>(src, s_w, s_r, n, ms, min_sep, margin, sparse, member_of, nullptr);
-    for (int i = threadIdx.x; i < n; i += blockDim.x) s_pos[i] = (i < stop && s_cent[i]) ? 1 : 0;
+    const int stop = merge_components<T>(src, s_w, s_r, n, ms, s_key, min_sep, sparse, member_of, nullptr);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s_pos[i] = (i < stop && ms.is_center[i]) ? 1 : 0;
     __syncthreads();
     const int n_out = block_exclusive_scan(s_pos, n, s_tmp);
     for (int i = threadIdx.x; i < n; i += blockDim.x)
-        if (i < stop && s_cent[i])
+        if (i < stop && ms.is_center[i])
             for (int q = 0; q < 28; ++q) out[(size_t)s_pos[i] * kRow + q] = sparse[(size_t)i * kRow + q];
     __syncthreads();
     // membership: centre index -> output row

@@ -120,10 +120,12 @@ def scene_seed(config_index: int, filter_index: int = 0) -> int:
 # ------------------------------------------------------------------ configurations
 WORKLOADS = {
     # name: (parents, landmarks, clutter rate, max Gaussians/parent, frames, max measurements)
-    "plain_c0": dict(n_parents=256, n_landmarks=50, clutter=10.0, max_gaussians=64, frames=100, max_meas=128),
-    "plain_c1": dict(n_parents=4096, n_landmarks=200, clutter=50.0, max_gaussians=256, frames=500, max_meas=384),
+    "plain_c0": dict(n_parents=256, n_landmarks=50, clutter=10.0, max_gaussians=64, frames=100, max_meas=128,
+                     max_survivors=384),
+    "plain_c1": dict(n_parents=4096, n_landmarks=200, clutter=50.0, max_gaussians=256, frames=500, max_meas=384,
+                     max_survivors=768),
     "precision_c3": dict(n_parents=16384, n_landmarks=400, clutter=100.0, max_gaussians=512, frames=300,
-                         max_meas=768),
+                         max_meas=768, max_survivors=1536),
 }
 
 
@@ -183,4 +185,5 @@ def workload(name: str, precision: int = 0, filter_index: int = 0, n_frames: Opt
     sc = make_scene(w["n_landmarks"], n_frames or w["frames"], w["clutter"], sd)
     cfg = filter_config(w["n_parents"], w["max_gaussians"], w["max_meas"], w["clutter"], precision,
                         calib=sc.calib, seed=sd)
+    cfg.max_survivors = w["max_survivors"]
     return sc, cfg
