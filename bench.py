@@ -361,7 +361,11 @@ def run_b200(args):
         "cpu_baseline": cpu,
         "clocks": clk,
         "counters": {"map_truncations": int(c1[0] - c0[0]), "scratch_overflows": int(c1[1]),
-                     "max_survivors_per_parent": int(c1[13]), "max_survivors_capacity": int(cfg.max_survivors)},
+                     "max_survivors_per_parent": int(c1[13]), "max_survivors_capacity": int(cfg.max_survivors),
+                     "clouds_read_per_parent_frame": float(c1[8] - c0[8]) / (K * cfg.n_parents),
+                     "clouds_written_per_parent_frame": float(c1[9] - c0[9]) / (K * cfg.n_parents),
+                     "fitted_per_parent_frame": float(c1[10] - c0[10]) / (K * cfg.n_parents),
+                     "merged_per_parent_frame": float(c1[11] - c0[11]) / (K * cfg.n_parents)},
     }
     print(json.dumps(line), flush=True)
     filt.close()

@@ -223,6 +223,39 @@ scphd_status scphd_merge_components_static(const double* comps, const uint8_t* f
 scphd_status scphd_systematic_resample(const double* weights, int32_t n, double u01,
                                        int32_t* idx);
 
+/* ------------------------------------------------------------------ batches
+ * Many filters advanced together: every batched step runs predict(dt) + update +
+ * resample for all member filters with one kernel launch per stage (six per frame,
+ * whatever the number of filters), each launch covering every filter's parents
+ * through a block -> (filter, parent) map.  Member filters must share device,
+ * precision and meas_dim; they may differ in size.  While in a batch, the filters
+ * issue all their work on the batch's stream (their own stream is restored by
+ * scphd_batch_destroy), so single-filter calls stay ordered with batched steps.  With
+ * use_graph != 0 the first step captures the step into a CUDA graph and later steps
+ * replay it.  A batched step gives each filter the same result as predict + update +
+ * resample on that filter alone.  This batching has no counterpart in the reference
+ * (which runs one filter per process). */
+typedef struct scphd_frame {
+    const double* u;        /* n measurements */
+    const double* v;
+    const double* d;        /* NULL in (u,v) mode */
+    int32_t n;
+    int32_t fixed_camera;
+} scphd_frame;
+
+typedef struct scphd_batch scphd_batch;
+
+scphd_status scphd_batch_create(scphd_filter* const* filters, int32_t n_filters, int32_t use_graph,
+                                scphd_batch** out);
+scphd_status scphd_batch_destroy(scphd_batch* b);
+/* frames[i] is filter i's frame; arrays in HOST memory (copied during the call). */
+scphd_status scphd_batch_step(scphd_batch* b, double dt, const scphd_frame* frames);
+/* As scphd_batch_step with the frames' arrays in DEVICE memory (read by the kernels;
+ * keep them unchanged until the step has run on the batch's stream). */
+scphd_status scphd_batch_step_device(scphd_batch* b, double dt, const scphd_frame* frames);
+/* The batch's CUDA stream (a cudaStream_t). */
+void* scphd_batch_stream(scphd_batch* b);
+
 /* Text of the last error on this thread. */
 const char* scphd_last_error(void);
 

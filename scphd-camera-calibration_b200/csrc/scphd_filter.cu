@@ -8,6 +8,7 @@
 
 #include <atomic>
 #include <cmath>
+#include <algorithm>
 #include <mutex>
 #include <cstdio>
 #include <cstring>
@@ -42,6 +43,22 @@ scphd_status fail(scphd_status s, const std::string& msg) {
 
 int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
+// The dynamic shared-memory limit is an attribute of the kernel function, shared by
+// every filter, batch and call in the process: it is raised to the device's whole
+// opt-in budget (less the kernel's static shared memory), so that no later setting
+// for a smaller launch can undercut a larger one.  The limit does not change the
+// occupancy of a launch, which follows the bytes that launch asks for.
+cudaError_t allow_dynamic_smem(const void* fn) {
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa{};
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, fn);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+    return e;
+}
+
 struct Arena {
     char* base = nullptr;
     size_t used = 0, cap = 0;
@@ -68,6 +85,8 @@ struct scphd_filter {
     uint32_t pending_frame = 0;
     uint32_t sample_frame[2] = {0, 0};
     int last_M = 0;
+    cudaStream_t own_stream = nullptr;   // the handle's stream while the filter is in a batch
+    void* batch = nullptr;               // the batch this filter belongs to, if any
     // opt-in per-stage event timing
     bool profiling = false;
     struct Mark { int stage; cudaEvent_t a, b; };
@@ -131,25 +150,10 @@ struct scphd_filter {
 
 namespace {
 
-template <typename T> __global__ void k_convert_meas(const double* stage, int M, int has_d, T* z) {
-    int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= M) return;
-    z[m * 3 + 0] = (T)stage[m];
-    z[m * 3 + 1] = (T)stage[M + m];
-    z[m * 3 + 2] = has_d ? (T)stage[2 * M + m] : T(0);
-}
-
 __global__ void k_iota(int* a, int n) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) a[i] = i;
 }
-
-__global__ void record_fit_n(const int* map_n, const int* src, int* fit_n, int n) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) fit_n[i] = map_n[src[i]];
-}
-
-__global__ void k_bump(unsigned long long* c, int i) { c[i] += 1; }
 
 __global__ void k_reset_src(int* src, int n) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -161,7 +165,6 @@ public:
     Bufs<T> b{};
     void* arena_ptr = nullptr;
     T* dump = nullptr;        // Gcap x 7 x Ps cloud dump scratch
-    int* fit_n = nullptr;     // N: Gaussians fitted at the last update
     size_t merge_smem = 0;
 
     ~Filter() override {
@@ -203,7 +206,7 @@ public:
         b.resample_idx = a.take<int>(N);
         b.counters = a.take<unsigned long long>(16);
         dump = a.take<T>(G * 7 * Ps);
-        fit_n = a.take<int>(N);
+        b.fit_n = a.take<int>(N);
         d_stage = a.take<double>(Mc * 3);
     }
 
@@ -229,9 +232,9 @@ public:
             return fail(SCPHD_ERR_CAPACITY, "max_survivors/max_gaussians need " + std::to_string(merge_smem) +
                                                 " bytes of shared memory per merge block (limit 227 KB)");
         if (prm.K == 2) {
-            CUDA_TRY(cudaFuncSetAttribute(k_merge<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem));
+            CUDA_TRY(allow_dynamic_smem((const void*)k_merge<T, 2>));
         } else {
-            CUDA_TRY(cudaFuncSetAttribute(k_merge<T, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)merge_smem));
+            CUDA_TRY(allow_dynamic_smem((const void*)k_merge<T, 3>));
         }
         const int N = prm.N;
         k_prior<<<(N + 255) / 256, 256, 0, stream>>>(prm, b.ext, b.lw);
@@ -276,12 +279,9 @@ public:
         const int N = prm.N;
         CUDA_TRY(cudaMemsetAsync(b.counters + 4, 0, 2 * sizeof(unsigned long long), stream));
         int h = stage_begin(1);
-        if (prm.P <= 128)
-            k_cloud_fit<T, K, 4><<<N, 256, 0, stream>>>(prm, b, cur, M, fixed, pending ? 1 : 0, pending_dt,
-                                                         pending_frame, sample_frame[cur]);
-        else
-            k_cloud_fit<T, K, 8><<<N, 256, 0, stream>>>(prm, b, cur, M, fixed, pending ? 1 : 0, pending_dt,
-                                                         pending_frame, sample_frame[cur]);
+        k_cloud_fit<T, K><<<N, 256, 0, stream>>>(prm, b, cur, M, fixed, pending ? 1 : 0, pending_dt, pending_frame,
+                                                  sample_frame[cur], M > 0 ? d_stage : nullptr,
+                                                  M > 0 ? d_stage + M : nullptr, M > 0 ? d_stage + 2 * M : nullptr);
         LAUNCHED();
         stage_end(h);
         pending = false;
@@ -297,36 +297,21 @@ public:
         LAUNCHED();
         stage_end(h);
         h = stage_begin(4);
-        k_weights<<<1, 1024, 0, stream>>>(N, b.lw, b.loglik, fixed ? 0 : 1, b.scal);
+        k_weights<<<1, 1024, 0, stream>>>(N, b.lw, b.loglik, fixed ? 0 : 1, b.scal, b.counters);
         LAUNCHED();
         stage_end(h);
         return SCPHD_OK;
     }
 
+    // one update: the kernels convert the staged measurements, record the fitted
+    // counts, reset the src indirection and count the frame themselves
     scphd_status update_staged(int M, int fixed) override {
-        if (M > 0) {
-            k_convert_meas<T><<<(M + 127) / 128, 128, 0, stream>>>(d_stage, M, prm.K == 3 ? 1 : 0, b.z);
-            LAUNCHED();
-        }
-        // fit_n[p] = G_p for the inspection dumps (taken from the prior map)
         scphd_status s = prm.K == 2 ? update_k<2>(M, fixed) : update_k<3>(M, fixed);
         if (s != SCPHD_OK) return s;
-        const int N = prm.N;
-        // fitted counts: the map sizes the update consumed
-        record_fit_n<<<(N + 255) / 256, 256, 0, stream>>>(b.map_n[cur], b.src, fit_n, N);
-        LAUNCHED();
         cur ^= 1;
         sample_frame[cur] = frame;
-        k_reset_src<<<(N + 255) / 256, 256, 0, stream>>>(b.src, N);
-        LAUNCHED();
         last_M = M;
-        bump_counter(2);
         return SCPHD_OK;
-    }
-
-    void bump_counter(int i) {
-        k_bump<<<1, 1, 0, stream>>>(b.counters, i);
-        g_launches.fetch_add(1, std::memory_order_relaxed);
     }
 
     scphd_status resample(int32_t* resampled, bool read_back) override {
@@ -410,7 +395,7 @@ public:
         const T* base;
         int width;
         if (which == SCPHD_MIX_FITTED) {
-            CUDA_TRY(cudaMemcpyAsync(&cnt, fit_n + p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+            CUDA_TRY(cudaMemcpyAsync(&cnt, b.fit_n + p, sizeof(int), cudaMemcpyDeviceToHost, stream));
             base = b.fit + (size_t)p * prm.Gcap * kRow;
             width = 29;
         } else if (which == SCPHD_MIX_MERGED) {
@@ -617,6 +602,7 @@ scphd_status scphd_create(const scphd_config* cfg, scphd_filter** out) {
 
 scphd_status scphd_destroy(scphd_filter* f) {
     if (!f) return fail(SCPHD_ERR_INVALID, "null handle");
+    if (f->batch) return fail(SCPHD_ERR_INVALID, "filter is in a batch: destroy the batch first");
     cudaSetDevice(f->cfg.device);
     delete f;
     return SCPHD_OK;
@@ -793,7 +779,7 @@ scphd_status scphd_merge_components(const double* comps, const uint8_t* flags, i
             cudaMemcpy(d_rows, rows.data(), sizeof(T) * rows.size(), cudaMemcpyHostToDevice);
             cudaMemcpy(d_flags, flags, n, cudaMemcpyHostToDevice);
             cudaMemset(d_mem, 0xff, sizeof(int) * n);
-            cudaFuncSetAttribute(k_merge_list<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            allow_dynamic_smem((const void*)k_merge_list<T>);
             k_merge_list<T><<<1, 128, smem>>>(d_rows, d_flags, n, (T)min_separation, d_sparse, d_out, d_n, d_mem);
             g_launches.fetch_add(1, std::memory_order_relaxed);
             cudaError_t e = cudaDeviceSynchronize();
@@ -898,7 +884,7 @@ scphd_status merge_static_impl(unsigned char* base, const double* comps, const u
     k_rows_from28<T><<<(n * kRow + 255) / 256, 256>>>(d_in, n, d_rows);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     const size_t smem = merge_smem_bytes<T>(n + 1, 0, 4);
-    CUDA_TRY(cudaFuncSetAttribute(k_merge_list<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUDA_TRY(allow_dynamic_smem((const void*)k_merge_list<T>));
     k_merge_list<T><<<1, 128, smem>>>(d_rows, d_flags, n, (T)min_separation, d_sparse, d_out, d_cnt, d_mem);
     g_launches.fetch_add(1, std::memory_order_relaxed);
     k_rows_to28<T><<<(n * 28 + 255) / 256, 256>>>(d_out, d_cnt, d_out28);
@@ -994,5 +980,274 @@ scphd_status scphd_get_stage_times(scphd_filter* f, double ms[8], int64_t launch
 const char* scphd_last_error(void) { return g_err.c_str(); }
 
 int64_t scphd_kernel_launches(void) { return g_launches.load(); }
+
+}  // extern "C"
+
+// ====================================================================== batches
+struct scphd_batch {
+    cudaStream_t stream = nullptr;
+    std::vector<scphd_filter*> fs;
+    virtual ~scphd_batch() {}
+    virtual scphd_status step(double dt, const scphd_frame* frames, bool device_frames) = 0;
+};
+
+namespace {
+
+template <typename T> struct Batch final : scphd_batch {
+    int K = 3;
+    bool use_graph = false;
+    bool captured = false;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t done = nullptr;
+    Slot<T>* h_slots = nullptr;   // pinned
+    Slot<T>* d_slots = nullptr;
+    double* h_stage = nullptr;    // pinned, 3 x Mcap per filter
+    double* d_stage = nullptr;
+    std::vector<size_t> stage_off;
+    size_t stage_total = 0;
+    int2* d_map_parent = nullptr; int n_parent_ctas = 0;
+    int2* d_map_pred = nullptr;   int n_pred_ctas = 0;
+    int4* d_map_lik = nullptr;    int n_lik_ctas = 0;
+    size_t merge_smem = 0;
+    void* dev_mem = nullptr;
+
+    ~Batch() override {
+        if (stream) cudaStreamSynchronize(stream);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (done) cudaEventDestroy(done);
+        if (h_slots) cudaFreeHost(h_slots);
+        if (h_stage) cudaFreeHost(h_stage);
+        if (dev_mem) cudaFree(dev_mem);
+        for (scphd_filter* f : fs) {   // give the filters their own streams back
+            f->stream = f->own_stream;
+            f->own_stream = nullptr;
+            f->batch = nullptr;
+        }
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    Filter<T>* filt(size_t i) const { return static_cast<Filter<T>*>(fs[i]); }
+
+    scphd_status init(bool graph) {
+        use_graph = graph;
+        const int F = (int)fs.size();
+        K = fs[0]->prm.K;
+        CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+        // block maps
+        std::vector<int2> mp, mpred;
+        std::vector<int4> ml;
+        stage_off.resize(F);
+        for (int f = 0; f < F; ++f) {
+            const Params& pr = fs[f]->prm;
+            for (int q = 0; q < pr.N; ++q) mp.push_back(make_int2(f, q));
+            for (int q = 0; q < pr.N; q += 256) mpred.push_back(make_int2(f, q));
+            const int mb = (pr.Mcap + 127) / 128;
+            for (int q = 0; q < pr.N; ++q)
+                for (int k = 0; k < mb; ++k) ml.push_back(make_int4(f, q, k, 0));
+            stage_off[f] = stage_total;
+            stage_total += 3 * (size_t)pr.Mcap;
+            merge_smem = std::max(merge_smem, merge_smem_bytes<T>(pr.Scap, pr.Gcap, 4));
+        }
+        n_parent_ctas = (int)mp.size();
+        n_pred_ctas = (int)mpred.size();
+        n_lik_ctas = (int)ml.size();
+        Arena probe;
+        probe.take<Slot<T>>(F);
+        probe.take<double>(stage_total);
+        probe.take<int2>(mp.size());
+        probe.take<int2>(mpred.size());
+        probe.take<int4>(ml.size());
+        CUDA_TRY(cudaMalloc(&dev_mem, probe.used));
+        Arena a;
+        a.base = static_cast<char*>(dev_mem);
+        d_slots = a.take<Slot<T>>(F);
+        d_stage = a.take<double>(stage_total);
+        d_map_parent = a.take<int2>(mp.size());
+        d_map_pred = a.take<int2>(mpred.size());
+        d_map_lik = a.take<int4>(ml.size());
+        CUDA_TRY(cudaMallocHost(&h_slots, sizeof(Slot<T>) * F));
+        CUDA_TRY(cudaMallocHost(&h_stage, sizeof(double) * std::max<size_t>(stage_total, 1)));
+        CUDA_TRY(cudaMemcpy(d_map_parent, mp.data(), sizeof(int2) * mp.size(), cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(d_map_pred, mpred.data(), sizeof(int2) * mpred.size(), cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(d_map_lik, ml.data(), sizeof(int4) * ml.size(), cudaMemcpyHostToDevice));
+        if (merge_smem > 227 * 1024) return fail(SCPHD_ERR_CAPACITY, "batch merge needs more than 227 KB of shared memory");
+        if (K == 2) {
+            CUDA_TRY(allow_dynamic_smem((const void*)k_merge_batch<T, 2>));
+        } else {
+            CUDA_TRY(allow_dynamic_smem((const void*)k_merge_batch<T, 3>));
+        }
+        // members now issue on the batch stream
+        for (scphd_filter* f : fs) {
+            CUDA_TRY(cudaStreamSynchronize(f->stream));
+            f->own_stream = f->stream;
+            f->stream = stream;
+            f->batch = this;
+        }
+        return SCPHD_OK;
+    }
+
+    template <int KK> scphd_status launch_all() {
+        const int F = (int)fs.size();
+        k_predict_parents_batch<T><<<n_pred_ctas, 256, 0, stream>>>(d_slots, d_map_pred);
+        LAUNCHED();
+        k_cloud_fit_batch<T, KK><<<n_parent_ctas, 256, 0, stream>>>(d_slots, d_map_parent);
+        LAUNCHED();
+        k_likelihood_batch<T, KK><<<n_lik_ctas, 128, 0, stream>>>(d_slots, d_map_lik);
+        LAUNCHED();
+        k_merge_batch<T, KK><<<n_parent_ctas, 128, merge_smem, stream>>>(d_slots, d_map_parent);
+        LAUNCHED();
+        k_weights_batch<T><<<F, 1024, 0, stream>>>(d_slots);
+        LAUNCHED();
+        k_resample_batch<T><<<F, 1024, 0, stream>>>(d_slots);
+        LAUNCHED();
+        return SCPHD_OK;
+    }
+
+    scphd_status enqueue() {
+        CUDA_TRY(cudaMemcpyAsync(d_stage, h_stage, sizeof(double) * stage_total, cudaMemcpyHostToDevice, stream));
+        CUDA_TRY(cudaMemcpyAsync(d_slots, h_slots, sizeof(Slot<T>) * fs.size(), cudaMemcpyHostToDevice, stream));
+        return K == 2 ? launch_all<2>() : launch_all<3>();
+    }
+
+    scphd_status step(double dt, const scphd_frame* frames, bool device_frames) override {
+        const int F = (int)fs.size();
+        for (int f = 0; f < F; ++f) {
+            const scphd_frame& fr = frames[f];
+            const Params& pr = fs[f]->prm;
+            if (fr.n < 0 || fr.n > pr.Mcap)
+                return fail(SCPHD_ERR_CAPACITY, "batch frame " + std::to_string(f) + ": bad measurement count");
+            if (fr.n > 0 && (!fr.u || !fr.v || (K == 3 && !fr.d)))
+                return fail(SCPHD_ERR_INVALID, "batch frame " + std::to_string(f) + ": null measurement array");
+            if (!device_frames)
+                for (int i = 0; i < fr.n; ++i)
+                    if (!std::isfinite(fr.u[i]) || !std::isfinite(fr.v[i]) || (K == 3 && !std::isfinite(fr.d[i])))
+                        return fail(SCPHD_ERR_INVALID, "non-finite measurement");
+        }
+        // the pinned buffers are rewritten: the previous step must have consumed them
+        CUDA_TRY(cudaEventSynchronize(done));
+        for (int f = 0; f < F; ++f) {
+            Filter<T>* fl = filt(f);
+            if (fl->pending) {   // a predict() issued outside the batch: apply it first
+                scphd_status s = fl->materialize_pending();
+                if (s != SCPHD_OK) return s;
+            }
+            const scphd_frame& fr = frames[f];
+            fl->frame++;
+            if (fl->frame >= (1u << 20)) return fail(SCPHD_ERR_CAPACITY, "frame counter exhausted (2^20 frames)");
+            Slot<T>& sl = h_slots[f];
+            sl.prm = fl->prm;
+            sl.b = fl->b;
+            FrameArgs& fa = sl.fa;
+            fa.cur = fl->cur;
+            fa.M = fr.n;
+            fa.fixed = fr.fixed_camera ? 1 : 0;
+            fa.has_pred = 1;
+            fa.dt = dt;
+            fa.pred_frame = fl->frame;
+            fa.sample_frame = fl->sample_frame[fl->cur];
+            fa.frame = fl->frame;
+            if (fr.n == 0) {
+                fa.zu = fa.zv = fa.zd = nullptr;
+            } else if (device_frames) {
+                fa.zu = fr.u;
+                fa.zv = fr.v;
+                fa.zd = K == 3 ? fr.d : nullptr;
+            } else {
+                double* hs = h_stage + stage_off[f];
+                std::memcpy(hs, fr.u, sizeof(double) * fr.n);
+                std::memcpy(hs + fr.n, fr.v, sizeof(double) * fr.n);
+                if (K == 3) std::memcpy(hs + 2 * fr.n, fr.d, sizeof(double) * fr.n);
+                const double* ds = d_stage + stage_off[f];
+                fa.zu = ds;
+                fa.zv = ds + fr.n;
+                fa.zd = K == 3 ? ds + 2 * fr.n : nullptr;
+            }
+        }
+        if (use_graph) {
+            if (!captured) {
+                cudaGraph_t g = nullptr;
+                CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+                scphd_status s = enqueue();
+                cudaError_t e = cudaStreamEndCapture(stream, &g);
+                if (s != SCPHD_OK) return s;
+                if (e != cudaSuccess) return fail(SCPHD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+                e = cudaGraphInstantiate(&exec, g, 0);
+                cudaGraphDestroy(g);
+                if (e != cudaSuccess) return fail(SCPHD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+                captured = true;
+                g_launches.fetch_sub(6, std::memory_order_relaxed);   // captured, not run: counted at replay
+            }
+            CUDA_TRY(cudaGraphLaunch(exec, stream));
+            g_launches.fetch_add(6, std::memory_order_relaxed);
+        } else {
+            scphd_status s = enqueue();
+            if (s != SCPHD_OK) return s;
+        }
+        CUDA_TRY(cudaEventRecord(done, stream));
+        for (int f = 0; f < F; ++f) {
+            Filter<T>* fl = filt(f);
+            fl->cur ^= 1;
+            fl->sample_frame[fl->cur] = fl->frame;
+            fl->pending = false;
+            fl->last_M = frames[f].n;
+        }
+        return SCPHD_OK;
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+scphd_status scphd_batch_create(scphd_filter* const* filters, int32_t n, int32_t use_graph, scphd_batch** out) {
+    if (!out || !filters || n < 1) return fail(SCPHD_ERR_INVALID, "bad batch arguments");
+    *out = nullptr;
+    const scphd_config& c0 = filters[0]->cfg;
+    for (int i = 0; i < n; ++i) {
+        if (!filters[i]) return fail(SCPHD_ERR_INVALID, "null filter in batch");
+        const scphd_config& c = filters[i]->cfg;
+        if (c.device != c0.device || c.precision != c0.precision || c.meas_dim != c0.meas_dim)
+            return fail(SCPHD_ERR_INVALID, "batch members must share device, precision and meas_dim");
+        if (filters[i]->batch) return fail(SCPHD_ERR_INVALID, "filter already in a batch");
+        for (int j = 0; j < i; ++j)
+            if (filters[j] == filters[i]) return fail(SCPHD_ERR_INVALID, "filter listed twice");
+    }
+    CUDA_TRY(cudaSetDevice(c0.device));
+    scphd_batch* b = c0.precision == SCPHD_FP64 ? static_cast<scphd_batch*>(new Batch<double>())
+                                                : static_cast<scphd_batch*>(new Batch<float>());
+    b->fs.assign(filters, filters + n);
+    scphd_status s = c0.precision == SCPHD_FP64 ? static_cast<Batch<double>*>(b)->init(use_graph != 0)
+                                                : static_cast<Batch<float>*>(b)->init(use_graph != 0);
+    if (s != SCPHD_OK) {
+        delete b;
+        return s;
+    }
+    *out = b;
+    return SCPHD_OK;
+}
+
+scphd_status scphd_batch_destroy(scphd_batch* b) {
+    if (!b) return fail(SCPHD_ERR_INVALID, "null batch");
+    cudaSetDevice(b->fs[0]->cfg.device);
+    delete b;
+    return SCPHD_OK;
+}
+
+scphd_status scphd_batch_step(scphd_batch* b, double dt, const scphd_frame* frames) {
+    if (!b || !frames) return fail(SCPHD_ERR_INVALID, "null batch or frames");
+    if (!std::isfinite(dt)) return fail(SCPHD_ERR_INVALID, "dt must be finite");
+    CUDA_TRY(cudaSetDevice(b->fs[0]->cfg.device));
+    return b->step(dt, frames, false);
+}
+
+scphd_status scphd_batch_step_device(scphd_batch* b, double dt, const scphd_frame* frames) {
+    if (!b || !frames) return fail(SCPHD_ERR_INVALID, "null batch or frames");
+    if (!std::isfinite(dt)) return fail(SCPHD_ERR_INVALID, "dt must be finite");
+    CUDA_TRY(cudaSetDevice(b->fs[0]->cfg.device));
+    return b->step(dt, frames, true);
+}
+
+void* scphd_batch_stream(scphd_batch* b) { return b ? (void*)b->stream : nullptr; }
 
 }  // extern "C"

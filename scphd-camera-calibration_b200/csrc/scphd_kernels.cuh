@@ -59,6 +59,24 @@ template <typename T> struct Bufs {
     int* flags;         // [0] resampled
     int* resample_idx;  // N
     unsigned long long* counters;   // 16
+    int* fit_n;         // N: Gaussians the last update fitted (prior map size)
+};
+
+// Per-filter arguments of one frame's kernels.
+struct FrameArgs {
+    int cur, M, fixed, has_pred;
+    double dt;
+    uint32_t pred_frame, sample_frame, frame;
+    const double* zu;   // this frame's measurements (FP64, device; zd unused in (u,v) mode)
+    const double* zv;
+    const double* zd;
+};
+
+// One filter of a batch: its constants, buffers and frame arguments.
+template <typename T> struct Slot {
+    Params prm;
+    Bufs<T> b;
+    FrameArgs fa;
 };
 
 __device__ __forceinline__ uint32_t tie_key(uint32_t r) {
@@ -90,8 +108,8 @@ __device__ inline double wrap_angle(double a) {   // src/device_math.cu:308-318
     return r;
 }
 
-__global__ void k_predict_parents(Params prm, double* ext, double dt, uint32_t frame) {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void predict_parents_body(const Params& prm, double* ext, double dt, uint32_t frame,
+                                                     int p) {
     if (p >= prm.N) return;
     double z[8];
     for (int b = 0; b < 2; ++b) {
@@ -110,21 +128,47 @@ __global__ void k_predict_parents(Params prm, double* ext, double dt, uint32_t f
     for (int q = 0; q < 3; ++q) e[6 + q] = wrap_angle(e[6 + q]);
 }
 
+__global__ void k_predict_parents(__grid_constant__ const Params prm, double* ext, double dt, uint32_t frame) {
+    predict_parents_body(prm, ext, dt, frame, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // ---------------------------------------------------------------- (b) cloud -> fit
 // One CTA per parent, one warp per daughter Gaussian; lane l owns samples
-// l, l+32, ... (NS per lane).  Covers: predict_features + ps (.cu:154-178,
-// 1144-1150), worldToDisparityKernel + computePdKernel (kernels.cu:6-47, 82-99),
-// weight by pD (.cu:1602-1609), normalizeWeightsKernel + fitGaussiansKernel
-// (kernels.cu:996-1018, 102-438) and the non-detection copy (.cu:1290-1420).
-template <typename T, int K, int NS>
-__global__ void __launch_bounds__(256) k_cloud_fit(Params prm, Bufs<T> b, int cur, int M, int fixed,
-                                                   int has_pred, double dt, uint32_t pred_frame,
-                                                   uint32_t sample_frame) {
-    const int p = blockIdx.x;
+// l, l+32, ... .  Covers: predict_features + ps (.cu:154-178, 1144-1150),
+// worldToDisparityKernel + computePdKernel (kernels.cu:6-47, 82-99), weight by pD
+// (.cu:1602-1609), normalizeWeightsKernel + fitGaussiansKernel (kernels.cu:996-1018,
+// 102-438) and the non-detection copy (.cu:1290-1420).
+//
+// Samples stream through registers: each is generated (merged component: drawn from
+// its stored Gaussian with the counter-based stream; non-detection cloud: loaded),
+// predicted, transformed, and folded into one-pass moments about a shift (the
+// warp's first sample).  With w'_s = omega_s pD_s and S0 = sum w', the reference's
+// normalised weights are w'_s / S0, so mean = shift + S1/S0 and the weighted
+// covariance is (SS/S0 - d d') (1 + S2/S0^2) with d = S1/S0, S2 = sum w'^2 (the
+// (W^2 + SS)/W normaliser of kernels.cu:196 with W = 1).  When S0 = 0 the
+// reference weights every sample by 1; that fit matters only when the mean pD is
+// positive (some sample weight omega = 0), and is then recomputed in a second pass.
+// A non-detection cloud is kept only if W (1 - pD_mean) >= min_weight, which needs
+// W >= min_weight: clouds with W >= min_weight are written while streaming and the
+// new map references only the retained ones.
+template <typename T, int K>
+__device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>& b, int cur, int M, int fixed,
+                                               int has_pred, double dt, uint32_t pred_frame, uint32_t sample_frame,
+                                               const double* zu, const double* zv, const double* zd, int p) {
+    if (p == 0 && zu != nullptr) {   // this frame's measurements into the T layout (u, v, d)
+        for (int mm = threadIdx.x; mm < M; mm += blockDim.x) {
+            b.z[mm * 3 + 0] = (T)zu[mm];
+            b.z[mm * 3 + 1] = (T)zv[mm];
+            b.z[mm * 3 + 2] = (K == 3 && zd) ? (T)zd[mm] : T(0);
+        }
+    }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int row = b.src[p];
-    const int G = b.map_n[cur][row];
+    const int G = min(b.map_n[cur][row], prm.Gcap);
     __shared__ Pose<T> pose_upd, pose_src;
+    __shared__ int s_rd, s_wr;
+    __shared__ T s_km[8 * 72];   // per warp: P[21], S^-1[6], K[18], P'[21]
+    __shared__ T s_L[8 * 24];    // per warp: Cholesky factor of a merged component
     if (threadIdx.x == 0) {
         double zero[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         pose_upd = make_pose<T>(fixed ? zero : b.ext + 12 * p);
@@ -132,147 +176,179 @@ __global__ void __launch_bounds__(256) k_cloud_fit(Params prm, Bufs<T> b, int cu
         b.surv_n[p] = 0;
         atomicAdd(&b.counters[4], (unsigned long long)G * (unsigned long long)M);
         atomicAdd(&b.counters[6], (unsigned long long)G * (unsigned long long)M);
+        s_rd = 0;
+        s_wr = 0;
     }
     __syncthreads();
     const Model& m = prm.model;
     const int P = prm.P, Ps = prm.Ps;
     const T invP = T(1) / T(P);
-    __shared__ int s_rd, s_wr;
-    __shared__ T s_km[8 * 72];   // per warp: P[21], S^-1[6], K[18], P'[21]
-    if (threadIdx.x == 0) { s_rd = 0; s_wr = 0; }
-    __syncthreads();
+    const T dtT = (T)dt, half_dt2 = T(0.5) * (T)dt * (T)dt;
+    T* Lw = s_L + warp * 24;
     for (int j = warp; j < G; j += blockDim.x >> 5) {
         const size_t erow = (size_t)row * prm.Gcap + j;
         const T* ent = b.map[cur] + erow * kRow;
         const int ref = b.map_ref[cur][erow];
-        T W = ent[0];
-        T X[NS][6], om[NS];
-        if (lane == 0 && ref >= 0) atomicAdd(&s_rd, 1);
-        if (ref < 0) {   // merged component: regenerate its sample cloud (.cu:640-690 + :1222-1286)
+        const T W = has_pred ? ent[0] * (T)prm.ps : ent[0];
+        const T* cl_in = ref >= 0 ? b.cloud[cur] + (size_t)ref * 7 * Ps : nullptr;
+        if (ref < 0) {
             T L[21];
             chol6(ent + 7, L);
-            const uint32_t key_i = (uint32_t)(-1 - ref);
+            if (lane < 21) {
+                T v = L[0];
 #pragma unroll
-            for (int t = 0; t < NS; ++t) {
-                const int s = lane + 32 * t;
-                if (s < P) {
-                    uint32_t w0[4], w1[4];
-                    philox((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 0), prm.key0, prm.key1, w0);
-                    philox((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 1), prm.key0, prm.key1, w1);
-                    T z[6];
-                    Pair<T>::two(w0[0], w0[1], z[0], z[1]);
-                    Pair<T>::two(w0[2], w0[3], z[2], z[3]);
-                    Pair<T>::two(w1[0], w1[1], z[4], z[5]);
-                    T y[6];
-#pragma unroll
-                    for (int a = 0; a < 6; ++a) {
-                        T v = 0;
-#pragma unroll
-                        for (int c = 0; c <= a; ++c) v += L[tri(a, c)] * z[c];
-                        y[a] = v + ent[1 + a];
-                    }
-                    invert(y, pose_src, m, X[t]);
-                    om[t] = invP;
-                } else {
-#pragma unroll
-                    for (int a = 0; a < 6; ++a) X[t][a] = 0;
-                    om[t] = 0;
-                }
+                for (int i = 1; i < 21; ++i) if (lane == i) v = L[i];
+                Lw[lane] = v;
             }
-        } else {         // non-detection cloud carried from the previous frame
-            const T* cl = b.cloud[cur] + (size_t)ref * 7 * Ps;
-#pragma unroll
-            for (int t = 0; t < NS; ++t) {
-                const int s = lane + 32 * t;
-                if (s < P) {
-#pragma unroll
-                    for (int a = 0; a < 6; ++a) X[t][a] = cl[a * Ps + s];
-                    om[t] = cl[6 * Ps + s];
-                } else {
-#pragma unroll
-                    for (int a = 0; a < 6; ++a) X[t][a] = 0;
-                    om[t] = 0;
-                }
-            }
+            __syncwarp();
+        } else if (lane == 0) {
+            atomicAdd(&s_rd, 1);
         }
-        if (has_pred) {   // predict_features with feature noise, then w *= ps
-            W *= (T)prm.ps;
-            const T dtT = (T)dt, half_dt2 = T(0.5) * (T)dt * (T)dt;
+        const bool write_nd = W >= (T)prm.min_weight;
+        T* cl_out = b.cloud[cur ^ 1] + ((size_t)p * prm.Gcap + j) * 7 * Ps;
+        const uint32_t key_i = (uint32_t)(-1 - ref);
+        // sample s: world point after the pending prediction, and its sample weight
+        auto sample = [&](int s, T X[6], T& om) {
+            if (ref < 0) {   // merged component: draw (.cu:640-690) and map to world (.cu:1222-1286)
+                uint32_t w0[4], w1[4];
+                philox((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 0), prm.key0, prm.key1, w0);
+                philox((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 1), prm.key0, prm.key1, w1);
+                T z[6];
+                Pair<T>::two(w0[0], w0[1], z[0], z[1]);
+                Pair<T>::two(w0[2], w0[3], z[2], z[3]);
+                Pair<T>::two(w1[0], w1[1], z[4], z[5]);
+                T y[6];
 #pragma unroll
-            for (int t = 0; t < NS; ++t) {
-                const int s = lane + 32 * t;
-                if (s < P) {
-                    uint32_t w[4];
-                    philox((uint32_t)s, (uint32_t)j, (uint32_t)p, ctr_word3(pred_frame, ST_FEAT, 0), prm.key0, prm.key1, w);
-                    T z[4];
-                    Pair<T>::two(w[0], w[1], z[0], z[1]);
-                    Pair<T>::two(w[2], w[3], z[2], z[3]);
+                for (int a = 0; a < 6; ++a) {
+                    T v = 0;
 #pragma unroll
-                    for (int q = 0; q < 3; ++q) {
-                        T a = (T)prm.feat_std[q] * z[q];
-                        X[t][q] = X[t][q] + X[t][q + 3] * dtT + a * half_dt2;
-                        X[t][q + 3] = X[t][q + 3] + a * dtT;
-                    }
+                    for (int c = 0; c <= a; ++c) v += Lw[tri(a, c)] * z[c];
+                    y[a] = v + ent[1 + a];
+                }
+                invert(y, pose_src, m, X);
+                om = invP;
+            } else {         // non-detection cloud carried from the previous frame
+#pragma unroll
+                for (int a = 0; a < 6; ++a) X[a] = cl_in[a * Ps + s];
+                om = cl_in[6 * Ps + s];
+            }
+            if (has_pred) {   // predict_features with feature noise
+                uint32_t w[4];
+                philox((uint32_t)s, (uint32_t)j, (uint32_t)p, ctr_word3(pred_frame, ST_FEAT, 0), prm.key0, prm.key1, w);
+                T z[4];
+                Pair<T>::two(w[0], w[1], z[0], z[1]);
+                Pair<T>::two(w[2], w[3], z[2], z[3]);
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    T a = (T)prm.feat_std[q] * z[q];
+                    X[q] = X[q] + X[q + 3] * dtT + a * half_dt2;
+                    X[q + 3] = X[q + 3] + a * dtT;
                 }
             }
-        }
-        // world -> disparity, pD per sample, weight by pD
-        T y[NS][6], pds[NS];
-        T sum_om = 0;
+        };
+        T shift[6] = {0, 0, 0, 0, 0, 0};
+        T S0 = 0, S2 = 0, S1[6] = {0, 0, 0, 0, 0, 0}, SS[21];
+#pragma unroll
+        for (int i = 0; i < 21; ++i) SS[i] = 0;
         int n_in = 0;
-#pragma unroll
-        for (int t = 0; t < NS; ++t) {
+        for (int t = 0; t * 32 < P; ++t) {
             const int s = lane + 32 * t;
-            bool valid = s < P;
+            const bool valid = s < P;
+            T X[6], om = 0, y[6];
             if (valid) {
-                measure(X[t], pose_upd, m, y[t]);
+                sample(s, X, om);
+                measure(X, pose_upd, m, y);
             } else {
 #pragma unroll
-                for (int a = 0; a < 6; ++a) y[t][a] = 0;
+                for (int a = 0; a < 6; ++a) { X[a] = 0; y[a] = 0; }
             }
-            bool inr = valid && in_range(y[t], m);
-            pds[t] = inr ? (T)m.pd : T(0);
+            const bool inr = valid && in_range(y, m);
+            const T pds = inr ? (T)m.pd : T(0);
             n_in += __popc(__ballot_sync(0xffffffffu, inr));
-            om[t] *= pds[t];
-            sum_om += om[t];
-        }
-        sum_om = warp_sum(sum_om);
-        // normalise: exp(safeLog(w) - safeLog(sum)) -> w/sum, 0, or 1 when the sum is 0
-        T wsum = 0, wsq = 0, mu[6] = {0, 0, 0, 0, 0, 0};
+            if (t == 0) {   // shift: the warp's first sample (finite), else 0
 #pragma unroll
-        for (int t = 0; t < NS; ++t) {
-            const int s = lane + 32 * t;
-            T w = (s < P) ? ((sum_om > T(0)) ? om[t] / sum_om : T(1)) : T(0);
-            om[t] = w;
-            wsum += w;
-            wsq += w * w;
-            if (w != T(0)) {
+                for (int a = 0; a < 6; ++a) {
+                    T v = __shfl_sync(0xffffffffu, y[a], 0);
+                    shift[a] = isfinite(v) ? v : T(0);
+                }
+            }
+            if (valid && write_nd) {   // non-detection cloud candidate: predicted world point, weight 1 - pD
 #pragma unroll
-                for (int a = 0; a < 6; ++a) mu[a] += y[t][a] * w;
+                for (int a = 0; a < 6; ++a) cl_out[a * Ps + s] = X[a];
+                cl_out[6 * Ps + s] = T(1) - pds;
+            }
+            const T wp = om * pds;
+            if (wp != T(0)) {   // zero-weight samples do not enter the sums
+                T d[6];
+#pragma unroll
+                for (int a = 0; a < 6; ++a) d[a] = y[a] - shift[a];
+                S0 += wp;
+                S2 += wp * wp;
+#pragma unroll
+                for (int a = 0; a < 6; ++a) S1[a] += wp * d[a];
+#pragma unroll
+                for (int a = 0; a < 6; ++a)
+#pragma unroll
+                    for (int c = 0; c <= a; ++c) SS[tri(a, c)] += wp * d[a] * d[c];
             }
         }
-        wsum = warp_sum(wsum);
-        wsq = warp_sum(wsq);
+        if (write_nd && lane == 0) atomicAdd(&s_wr, 1);
+        S0 = warp_sum(S0);
+        S2 = warp_sum(S2);
 #pragma unroll
-        for (int a = 0; a < 6; ++a) mu[a] = warp_sum(mu[a]);
-        const T covscale = (wsum * wsum + wsq) / wsum;   // 1 / cov_normalizer (kernels.cu:196)
-        T cv[21];
+        for (int a = 0; a < 6; ++a) S1[a] = warp_sum(S1[a]);
 #pragma unroll
-        for (int i = 0; i < 21; ++i) cv[i] = 0;
+        for (int i = 0; i < 21; ++i) SS[i] = warp_sum(SS[i]);
+        const T pbar = (T)((double)n_in * m.pd / (double)P);
+        T mu[6], cv[21];
+        if (S0 > T(0)) {
+            const T inv = T(1) / S0, scale = T(1) + S2 * inv * inv;
+            T d[6];
 #pragma unroll
-        for (int t = 0; t < NS; ++t) {
-            if (om[t] == T(0)) continue;
-            T dv[6];
-#pragma unroll
-            for (int a = 0; a < 6; ++a) dv[a] = y[t][a] - mu[a];
+            for (int a = 0; a < 6; ++a) { d[a] = S1[a] * inv; mu[a] = shift[a] + d[a]; }
 #pragma unroll
             for (int a = 0; a < 6; ++a)
 #pragma unroll
-                for (int c = 0; c <= a; ++c) cv[tri(a, c)] += dv[a] * dv[c] * om[t];
-        }
+                for (int c = 0; c <= a; ++c) cv[tri(a, c)] = (SS[tri(a, c)] * inv - d[a] * d[c]) * scale;
+        } else if (pbar > T(0)) {
+            // every sample weighted 1 (exp(LOG0 - LOG0)): unnormalised mean and
+            // covariance x (P + P)/P over the valid samples
+            T U1[6] = {0, 0, 0, 0, 0, 0}, U2[21];
 #pragma unroll
-        for (int i = 0; i < 21; ++i) cv[i] = warp_sum(cv[i]) * covscale;
-        const T pbar = (T)((double)n_in * m.pd / (double)P);
+            for (int i = 0; i < 21; ++i) U2[i] = 0;
+            for (int t = 0; t * 32 < P; ++t) {
+                const int s = lane + 32 * t;
+                if (s < P) {
+                    T X[6], om, y[6];
+                    sample(s, X, om);
+                    measure(X, pose_upd, m, y);
+#pragma unroll
+                    for (int a = 0; a < 6; ++a) U1[a] += y[a];
+                }
+            }
+#pragma unroll
+            for (int a = 0; a < 6; ++a) mu[a] = warp_sum(U1[a]);   // sum of y (weights 1)
+            for (int t = 0; t * 32 < P; ++t) {
+                const int s = lane + 32 * t;
+                if (s < P) {
+                    T X[6], om, y[6];
+                    sample(s, X, om);
+                    measure(X, pose_upd, m, y);
+#pragma unroll
+                    for (int a = 0; a < 6; ++a)
+#pragma unroll
+                        for (int c = 0; c <= a; ++c) U2[tri(a, c)] += (y[a] - mu[a]) * (y[c] - mu[c]);
+                }
+            }
+            const T scale = (T(P) * T(P) + T(P)) / T(P);
+#pragma unroll
+            for (int i = 0; i < 21; ++i) cv[i] = warp_sum(U2[i]) * scale;
+        } else {   // entirely out of view: never used downstream (its log-constant is -inf)
+#pragma unroll
+            for (int a = 0; a < 6; ++a) mu[a] = shift[a];
+#pragma unroll
+            for (int i = 0; i < 21; ++i) cv[i] = 0;
+        }
         // fitted row: lane q writes element q (W, pD, mean[6], packed cov[21])
         T* fr = b.fit + ((size_t)p * prm.Gcap + j) * kRow;
         {
@@ -286,21 +362,6 @@ __global__ void __launch_bounds__(256) k_cloud_fit(Params prm, Bufs<T> b, int cu
         }
         warp_kalman_prep<T, K>(W, pbar, cv, m, s_km + warp * 72, lane,
                                b.prep + ((size_t)p * prm.Gcap + j) * kPrep);
-        // retained non-detection cloud: predicted world samples, weights 1 - pD
-        const T wnd = W * (T(1) - pbar);
-        if (wnd >= (T)prm.min_weight) {
-            if (lane == 0) atomicAdd(&s_wr, 1);
-            T* cl = b.cloud[cur ^ 1] + ((size_t)p * prm.Gcap + j) * 7 * Ps;
-#pragma unroll
-            for (int t = 0; t < NS; ++t) {
-                const int s = lane + 32 * t;
-                if (s < P) {
-#pragma unroll
-                    for (int a = 0; a < 6; ++a) cl[a * Ps + s] = X[t][a];
-                    cl[6 * Ps + s] = T(1) - pds[t];
-                }
-            }
-        }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -310,15 +371,33 @@ __global__ void __launch_bounds__(256) k_cloud_fit(Params prm, Bufs<T> b, int cu
     }
 }
 
+
+template <typename T, int K>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
+    k_cloud_fit(__grid_constant__ const Params prm, __grid_constant__ const Bufs<T> b, int cur, int M, int fixed,
+                int has_pred, double dt, uint32_t pred_frame, uint32_t sample_frame, const double* zu,
+                const double* zv, const double* zd) {
+    cloud_fit_body<T, K>(prm, b, cur, M, fixed, has_pred, dt, pred_frame, sample_frame, zu, zv, zd, blockIdx.x);
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_cloud_fit_batch(const Slot<T>* slots, const int2* map) {
+    const int2 fp = map[blockIdx.x];
+    const Slot<T>& sl = slots[fp.x];
+    const FrameArgs& fa = sl.fa;
+    cloud_fit_body<T, K>(sl.prm, sl.b, fa.cur, fa.M, fa.fixed, fa.has_pred, fa.dt, fa.pred_frame, fa.sample_frame,
+                         fa.zu, fa.zv, fa.zd, fp.y);
+}
+
 // ---------------------------------------------------------------- (c) likelihood
 // Normaliser ell_{p,m} = logsumexp_j(log w_{j,m}) (+) log(M w0 + kappa)
 // (.cu:1729-1768) and survivor compaction: w_{j,m} = exp(log w - ell) >= min_weight
 // with a PD posterior (updateKernel, kernels.cu:622-657), births likewise.
 template <typename T, int K>
-__global__ void __launch_bounds__(128) k_likelihood(Params prm, Bufs<T> b, int cur, int M) {
-    const int p = blockIdx.x;
-    const int m = blockIdx.y * blockDim.x + threadIdx.x;
-    const int G = b.map_n[cur][b.src[p]];
+__device__ __forceinline__ void likelihood_body(const Params& prm, const Bufs<T>& b, int cur, int M, int p,
+                                                int mblock) {
+    const int m = mblock * blockDim.x + threadIdx.x;
+    const int G = min(b.map_n[cur][b.src[p]], prm.Gcap);
     __shared__ T s_c[128], s_pd[128], s_si[128][6], s_mu[128][3];
     T zm[3] = {0, 0, 0};
     if (m < M) {
@@ -429,6 +508,21 @@ __global__ void __launch_bounds__(128) k_likelihood(Params prm, Bufs<T> b, int c
     }
 }
 
+template <typename T, int K>
+__global__ void __launch_bounds__(128) k_likelihood(__grid_constant__ const Params prm,
+                                                    __grid_constant__ const Bufs<T> b, int cur, int M) {
+    likelihood_body<T, K>(prm, b, cur, M, blockIdx.x, blockIdx.y);
+}
+
+// map entry: (filter, parent, measurement block); blocks past a filter's M exit
+template <typename T, int K>
+__global__ void __launch_bounds__(128) k_likelihood_batch(const Slot<T>* slots, const int4* map) {
+    const int4 e = map[blockIdx.x];
+    const Slot<T>& sl = slots[e.x];
+    if (e.z * (int)blockDim.x >= sl.fa.M) return;
+    likelihood_body<T, K>(sl.prm, sl.b, sl.fa.cur, sl.fa.M, e.y, e.z);
+}
+
 // ---------------------------------------------------------------- (d) merge
 // Component sources for the merge loop: posterior components of one parent
 // (detections and births), or an explicit list.
@@ -505,8 +599,10 @@ __device__ void sort_survivors(T* s_w, uint32_t* s_key, int* s_r, int n_pad) {
     }
 }
 
-// Block-wide exclusive scan of int flags (n <= blockDim * 64); returns the total.
+// Block-wide exclusive scan of int flags; returns the total.  Starts with a barrier:
+// callers write data in any pattern, each thread then scans a contiguous chunk.
 __device__ int block_exclusive_scan(int* data, int n, int* s_tmp) {
+    __syncthreads();
     const int per = (n + blockDim.x - 1) / blockDim.x;
     const int lo = threadIdx.x * per, hi = min(n, lo + per);
     int run = 0;
@@ -670,6 +766,47 @@ __device__ void merge_members_thread(const Src& src, const T* s_w, const int* s_
 #pragma unroll
         for (int e = 0; e < 21; ++e) o[7 + e] = ccov[e];
     }
+}
+
+// Order-preserving integer key of a non-negative weight.
+__device__ __forceinline__ uint64_t weight_key(float w) { return (uint64_t)__float_as_uint(w); }
+__device__ __forceinline__ uint64_t weight_key(double w) { return (uint64_t)__double_as_longlong(w); }
+
+// Exact k-th largest key among the entries with w >= 0 (k <= their count), by an
+// MSB-first radix select over 8-bit digits.  Block-wide call.
+template <typename T>
+__device__ uint64_t select_kth_largest(const T* w, int n, int k, int* s_tmp) {
+    __shared__ int s_hist[256];
+    __shared__ uint64_t s_prefix;
+    __shared__ int s_k;
+    const int passes = sizeof(T) == 4 ? 4 : 8;
+    uint64_t prefix = 0, mask = 0;
+    if (threadIdx.x == 0) s_k = k;
+    for (int d = passes - 1; d >= 0; --d) {
+        for (int b = threadIdx.x; b < 256; b += blockDim.x) s_hist[b] = 0;
+        __syncthreads();
+        for (int e = threadIdx.x; e < n; e += blockDim.x) {
+            const T v = w[e];
+            if (!(v >= T(0))) continue;
+            const uint64_t key = weight_key(v);
+            if ((key & mask) == prefix) atomicAdd(&s_hist[(key >> (8 * d)) & 255], 1);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int kk = s_k, b = 255;
+            for (; b > 0; --b) {
+                if (s_hist[b] >= kk) break;
+                kk -= s_hist[b];
+            }
+            s_k = kk;
+            s_prefix = prefix | ((uint64_t)b << (8 * d));
+        }
+        __syncthreads();
+        prefix = s_prefix;
+        mask |= (uint64_t)255 << (8 * d);
+    }
+    (void)s_tmp;
+    return prefix;
 }
 
 // In-place bitonic sort of (key, payload) ascending by key over n_pad (power of 2) slots.
@@ -964,11 +1101,10 @@ __device__ int merge_components(const Src& src, const T* s_w, const int* s_r, in
 }
 
 template <typename T, int K>
-__global__ void __launch_bounds__(128) k_merge(Params prm, Bufs<T> b, int cur, int M, int fixed) {
+__device__ __forceinline__ void merge_body(const Params& prm, const Bufs<T>& b, int cur, int M, int fixed, int p) {
     extern __shared__ __align__(16) unsigned char smem[];
-    const int p = blockIdx.x;
     const int tid = threadIdx.x;
-    const int G = b.map_n[cur][b.src[p]];
+    const int G = min(b.map_n[cur][b.src[p]], prm.Gcap);
     const int n_all_surv = b.surv_n[p];
     const int n = min(n_all_surv, prm.Scap);
     const int n_pad = next_pow2(n);
@@ -1055,20 +1191,34 @@ __global__ void __launch_bounds__(128) k_merge(Params prm, Bufs<T> b, int cur, i
     __syncthreads();
     const bool cut = s_nvalid > prm.Gcap;
     // keep: retained, and when over capacity among the Gcap largest (ties by entry order)
-    for (int e = tid; e < n_all; e += blockDim.x) {
-        const T w = s_w[e];
-        int keep = w >= T(0);
-        if (keep && cut) {
-            int rank = 0;
-            for (int f = 0; f < n_all; ++f) {
-                const T v = s_w[f];
-                rank += (v > w) || (v == w && f < e);
-            }
-            keep = rank < prm.Gcap;
+    if (!cut) {
+        for (int e = tid; e < n_all; e += blockDim.x) s_pos[e] = s_w[e] >= T(0);
+        __syncthreads();
+    } else {
+        const uint64_t thr = select_kth_largest(s_w, n_all, prm.Gcap, s_tmp);
+        // entries above the threshold, then ties in entry order up to Gcap
+        int above = 0;
+        for (int e = tid; e < n_all; e += blockDim.x) {
+            const T w = s_w[e];
+            const uint64_t key = w >= T(0) ? weight_key(w) : 0ull;
+            above += key > thr;
+            s_pos[e] = (w >= T(0) && key == thr) ? 1 : 0;
         }
-        s_pos[e] = keep;
+        __shared__ int s_above;
+        if (tid == 0) s_above = 0;
+        __syncthreads();
+        atomicAdd(&s_above, above);
+        __syncthreads();
+        const int ties_keep = prm.Gcap - s_above;
+        block_exclusive_scan(s_pos, n_all, s_tmp);   // rank among the ties
+        for (int e = tid; e < n_all; e += blockDim.x) {
+            const T w = s_w[e];
+            const uint64_t key = w >= T(0) ? weight_key(w) : 0ull;
+            const bool tie = w >= T(0) && key == thr;
+            s_pos[e] = (w >= T(0) && key > thr) || (tie && s_pos[e] < ties_keep);
+        }
+        __syncthreads();
     }
-    __syncthreads();
     const int total = block_exclusive_scan(s_pos, n_all, s_tmp);
     const int wrow = p;   // the new map lives at row p of the other buffer
     T* mo = b.map[cur ^ 1] + (size_t)wrow * prm.Gcap * kRow;
@@ -1089,7 +1239,7 @@ __global__ void __launch_bounds__(128) k_merge(Params prm, Bufs<T> b, int cur, i
     }
     if (tid == 0) {
         b.merged_n[p] = n_out;
-        b.map_n[cur ^ 1][wrow] = total;
+        b.map_n[cur ^ 1][wrow] = min(total, prm.Gcap);
         double* me = b.map_ext[cur ^ 1] + 12 * wrow;
         for (int q = 0; q < 12; ++q) me[q] = fixed ? 0.0 : b.ext[12 * p + q];
         if (cut) atomicAdd(&b.counters[0], 1ull);
@@ -1097,7 +1247,22 @@ __global__ void __launch_bounds__(128) k_merge(Params prm, Bufs<T> b, int cur, i
         atomicAdd(&b.counters[7], (unsigned long long)n);
         atomicAdd(&b.counters[11], (unsigned long long)n_out);
         atomicMax(&b.counters[13], (unsigned long long)n_all_surv);
+        b.fit_n[p] = G;   // prior map size, for the inspection dumps
+        b.src[p] = p;     // the new map lives at row p: the indirection is reset
     }
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(128) k_merge(__grid_constant__ const Params prm, __grid_constant__ const Bufs<T> b,
+                                               int cur, int M, int fixed) {
+    merge_body<T, K>(prm, b, cur, M, fixed, blockIdx.x);
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(128) k_merge_batch(const Slot<T>* slots, const int2* map) {
+    const int2 fp = map[blockIdx.x];
+    const Slot<T>& sl = slots[fp.x];
+    merge_body<T, K>(sl.prm, sl.b, sl.fa.cur, sl.fa.M, sl.fa.fixed, fp.y);
 }
 
 // ---------------------------------------------------------------- parent weights
@@ -1123,8 +1288,9 @@ __device__ double block_reduce_max(double v, double* s_tmp) {
 }
 
 // log-domain form of .cu:1845-1875: lw += loglik, normalise; N_eff of the result
-__global__ void __launch_bounds__(1024) k_weights(int N, double* lw, const double* loglik, int apply,
-                                                  double* scal) {
+__device__ __forceinline__ void weights_body(int N, double* lw, const double* loglik, int apply, double* scal,
+                                             unsigned long long* counters) {
+    if (threadIdx.x == 0 && counters) counters[2] += 1;   // frames updated
     __shared__ double s_tmp[32];
     double mx = -INFINITY;
     for (int p = threadIdx.x; p < N; p += blockDim.x) {
@@ -1146,6 +1312,17 @@ __global__ void __launch_bounds__(1024) k_weights(int N, double* lw, const doubl
     }
     ss = block_reduce_sum(ss, s_tmp);
     if (threadIdx.x == 0) scal[0] = 1.0 / (N * ss);   // computeNeff, .cu:2641-2649
+}
+
+__global__ void __launch_bounds__(1024) k_weights(int N, double* lw, const double* loglik, int apply, double* scal,
+                                                  unsigned long long* counters) {
+    weights_body(N, lw, loglik, apply, scal, counters);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024) k_weights_batch(const Slot<T>* slots) {
+    const Slot<T>& sl = slots[blockIdx.x];
+    weights_body(sl.prm.N, sl.b.lw, sl.b.loglik, sl.fa.fixed ? 0 : 1, sl.b.scal, sl.b.counters);
 }
 
 // ---------------------------------------------------------------- (e) resample
@@ -1184,10 +1361,10 @@ __device__ void block_scan_inclusive(double* data, int N, double* s_tmp) {
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(1024) k_resample(Params prm, double* lw, double* ext, double* ext_tmp,
-                                                   int* src, int* src_tmp, double* cum, double* scal,
-                                                   int* flags, int* idx_out, uint32_t frame, int force,
-                                                   double r0_override, unsigned long long* counters) {
+__device__ __forceinline__ void resample_body(const Params& prm, double* lw, double* ext, double* ext_tmp, int* src,
+                                              int* src_tmp, double* cum, double* scal, int* flags, int* idx_out,
+                                              uint32_t frame, int force, double r0_override,
+                                              unsigned long long* counters) {
     __shared__ double s_tmp[32];
     __shared__ double s_r0;
     __shared__ int s_amax;
@@ -1249,6 +1426,33 @@ __global__ void __launch_bounds__(1024) k_resample(Params prm, double* lw, doubl
     }
 }
 
+__global__ void __launch_bounds__(1024) k_resample(__grid_constant__ const Params prm, double* lw, double* ext,
+                                                   double* ext_tmp, int* src, int* src_tmp, double* cum, double* scal,
+                                                   int* flags, int* idx_out, uint32_t frame, int force,
+                                                   double r0_override, unsigned long long* counters) {
+    resample_body(prm, lw, ext, ext_tmp, src, src_tmp, cum, scal, flags, idx_out, frame, force, r0_override, counters);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024) k_resample_batch(const Slot<T>* slots) {
+    const Slot<T>& sl = slots[blockIdx.x];
+    const Bufs<T>& b = sl.b;
+    resample_body(sl.prm, b.lw, b.ext, b.ext_tmp, b.src, b.src_tmp, b.cum, b.scal, b.flags, b.resample_idx,
+                  sl.fa.frame, 0, -1.0, b.counters);
+}
+
+// map entry: (filter, first parent of a 256-parent block)
+template <typename T>
+__global__ void k_predict_parents_batch(const Slot<T>* slots, const int2* map) {
+    const int2 fp = map[blockIdx.x];
+    const Slot<T>& sl = slots[fp.x];
+    if (fp.y == 0 && threadIdx.x == 0) {   // counters of "the last update" start at 0
+        sl.b.counters[4] = 0;
+        sl.b.counters[5] = 0;
+    }
+    predict_parents_body(sl.prm, sl.b.ext, sl.fa.dt, sl.fa.frame, fp.y + threadIdx.x);
+}
+
 // ---------------------------------------------------------------- cloud materialisation
 // Write the Euclidean cloud of every entry of the maps into dst (rows p*Gcap + j),
 // optionally applying a pending feature prediction (the path of predict() called
@@ -1260,7 +1464,7 @@ __global__ void __launch_bounds__(256) k_materialize(Params prm, Bufs<T> b, int 
     const int p = only_p >= 0 ? only_p : blockIdx.x;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int row = b.src[p];
-    const int G = b.map_n[cur][row];
+    const int G = min(b.map_n[cur][row], prm.Gcap);
     __shared__ Pose<T> pose_src;
     if (threadIdx.x == 0) pose_src = make_pose<T>(b.map_ext[cur] + 12 * row);
     __syncthreads();

@@ -87,6 +87,12 @@ class ScphdConfig(ctypes.Structure):
         return out
 
 
+class ScphdFrame(ctypes.Structure):
+    """scphd_frame: one filter's measurements for a batched step."""
+    _fields_ = [("u", ctypes.c_void_p), ("v", ctypes.c_void_p), ("d", ctypes.c_void_p),
+                ("n", ctypes.c_int32), ("fixed_camera", ctypes.c_int32)]
+
+
 def reference_defaults() -> ScphdConfig:
     """The values of the reference's config/calibration.cfg, read the way its code
     reads them (the shipped {mean,std} prior becomes the box mean +- max(std, 0)),
@@ -166,6 +172,11 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "scphd_stream": (vp, [vp]),
         "scphd_set_profiling": (i32, [vp, i32]),
         "scphd_get_stage_times": (i32, [vp, P(d), P(i64)]),
+        "scphd_batch_create": (i32, [P(vp), i32, i32, P(vp)]),
+        "scphd_batch_destroy": (i32, [vp]),
+        "scphd_batch_step": (i32, [vp, d, P(ScphdFrame)]),
+        "scphd_batch_step_device": (i32, [vp, d, P(ScphdFrame)]),
+        "scphd_batch_stream": (vp, [vp]),
         "scphd_last_error": (ctypes.c_char_p, []),
         "scphd_kernel_launches": (i64, []),
     }
@@ -357,6 +368,75 @@ class SCPHDCameraCalibration:
         weights, clouds, omega = _f64(weights), _f64(clouds), _f64(omega)
         _check(self._lib.scphd_set_state(self._h, _dptr(states), _dptr(log_weights), _iptr(sizes),
                                          _dptr(weights), _dptr(clouds), _dptr(omega)))
+
+
+class SCPHDBatch:
+    """Several filters stepped together: one launch per stage for all of them
+    (scphd_batch_* in include/scphd.h).  Each member gets the result it would get
+    stepped alone.  The batch keeps its filters alive and returns them to their own
+    streams on close()."""
+
+    def __init__(self, filters: Sequence[SCPHDCameraCalibration], use_graph: bool = False):
+        self._lib = load_library()
+        self.filters = list(filters)
+        arr = (ctypes.c_void_p * len(self.filters))(*[f._h.value for f in self.filters])
+        h = ctypes.c_void_p()
+        _check(self._lib.scphd_batch_create(arr, len(self.filters), int(bool(use_graph)), ctypes.byref(h)))
+        self._h = h
+        self._frames = (ScphdFrame * len(self.filters))()
+        self._keep = []
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            _check(self._lib.scphd_batch_destroy(self._h))
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def step(self, dt: float, frames) -> None:
+        """frames: per filter (u, v, d or None, fixed_camera) host arrays."""
+        if len(frames) != len(self.filters):
+            raise ScphdError(1, "one frame per filter")
+        keep = []
+        for i, (u, v, d, fixed) in enumerate(frames):
+            u, v = _f64(u), _f64(v)
+            dd = _f64(d) if d is not None else None
+            if u.shape != v.shape or (dd is not None and dd.shape != u.shape):
+                raise ScphdError(1, "u, v (and d) must have the same length")
+            keep += [u, v, dd]
+            fr = self._frames[i]
+            fr.u, fr.v = u.ctypes.data, v.ctypes.data
+            fr.d = dd.ctypes.data if dd is not None else None
+            fr.n, fr.fixed_camera = int(u.size), int(bool(fixed))
+        _check(self._lib.scphd_batch_step(self._h, float(dt), self._frames))
+
+    def step_device(self, dt: float, frames) -> None:
+        """frames: per filter (u_ptr, v_ptr, d_ptr or None, n, fixed_camera) with FP64
+        device pointers that stay valid until the step has run on stream_handle()."""
+        if len(frames) != len(self.filters):
+            raise ScphdError(1, "one frame per filter")
+        for i, (u, v, d, n, fixed) in enumerate(frames):
+            fr = self._frames[i]
+            fr.u, fr.v, fr.d = int(u), int(v), (int(d) if d else None)
+            fr.n, fr.fixed_camera = int(n), int(bool(fixed))
+        _check(self._lib.scphd_batch_step_device(self._h, float(dt), self._frames))
+
+    def stream_handle(self) -> int:
+        return int(self._lib.scphd_batch_stream(self._h) or 0)
+
+    def synchronize(self) -> None:
+        for f in self.filters:
+            f.synchronize()
 
 
 def merge_components(comps: np.ndarray, flags: np.ndarray, min_separation: float,

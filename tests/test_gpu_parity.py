@@ -203,3 +203,38 @@ def test_fp32_frames_track_oracle(pkg, orc):
         assert rg == rr
         if rr and not np.array_equal(gpu.resample_indices(), ref.resample_indices()):
             break   # ancestries diverge from here on; the comparison ends
+
+
+@pytest.mark.parametrize("prec", [1, 0])
+def test_map_capacity_keeps_largest_weights(pkg, orc, prec):
+    """max_gaussians binds: the new map holds the max_gaussians largest weights of
+    (merged components, retained non-detection terms), ties in entry order, and
+    keeps the entries' order."""
+    _need_gpu()
+    sc = pkg.scene.make_scene(n_landmarks=30, n_frames=5, clutter_rate=6.0, seed=pkg.scene.scene_seed(0, 21))
+    cfg = pkg.scene.filter_config(n_parents=16, max_gaussians=12, max_meas=96, clutter_rate=6.0,
+                                  precision=prec, calib=sc.calib, seed=21, particles_per_feature=32)
+    gpu = pkg.SCPHDCameraCalibration(cfg)
+    hit = False
+    for k in range(sc.n_frames):
+        z = sc.frames[k]
+        gpu.predict(pkg.scene.DT)
+        gpu.update(z[:, 0], z[:, 1], fixed_camera=sc.fixed[k], d=z[:, 2])
+        sizes = gpu.map_sizes()
+        assert np.all(sizes <= 12)
+        for p in range(4):
+            mg = gpu.mixture(1, p)
+            fr = gpu.mixture(0, p)
+            wnd = fr[:, 0] * (1 - fr[:, 1])
+            cand = np.concatenate([mg[:, 0], np.where(wnd >= cfg.min_weight, wnd, -1.0)])
+            valid = np.where(cand >= 0)[0]
+            if valid.size > 12:
+                hit = True
+                order = sorted(valid, key=lambda e: (-cand[e], e))[:12]
+                keep = np.sort(order)
+            else:
+                keep = valid
+            np.testing.assert_allclose(gpu.map_weights(p), cand[keep], rtol=1e-6)
+        gpu.resample()
+    assert hit, "the capacity never bound in this scene"
+    assert gpu.counters()[0] > 0
