@@ -373,6 +373,131 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+def run_batched(args, pkg, quiet=False):
+    """Many-filter workload: 64 filters of uneven size (batched_specs), grouped into
+    device-resident waves under an 80% HBM budget.  Each wave is one SCPHDBatch
+    stepped from a captured CUDA graph (six kernels per frame for all its filters).
+    Timed per wave: K pairs of batched frames alternating with K pairs of frames in
+    which the same filters are stepped plain, one filter at a time (device events on
+    the batch stream), then K batched frames end to end from host arrays with the
+    parent states read back.  Rates are all waves' units over all waves' times."""
+    import torch
+    dev = torch.device("cuda", 0)
+    prec = pkg.SCPHD_FP32 if args.precision == "fp32" else pkg.SCPHD_FP64
+    K, W, PF = args.steps, args.warmup, args.prefill
+    n_pairs = max(1, (K + 1) // 2)
+    n_frames = PF + W + 4 * n_pairs + K
+    if args.workload == "batched_c0x64":
+        # the single-filter workload plain_c0 (256 parents, 50 landmarks, clutter 10,
+        # <= 64 Gaussians), 64 filters on their own seeded scenes
+        specs = [dict(index=i, n_parents=256, n_landmarks=50, clutter=10.0) for i in range(args.filters)]
+        built = [pkg.scene.spec_filter(sp, n_frames, prec, max_gaussians=64, config_index=0,
+                                       survivors_per_gaussian=6) for sp in specs]
+    else:
+        specs = pkg.scene.batched_specs(args.filters)
+        built = [pkg.scene.spec_filter(sp, n_frames, prec) for sp in specs]
+    sizes = [pkg.device_bytes(cfg) for _, cfg in built]
+    free, total = torch.cuda.mem_get_info(dev)
+    budget = int(0.8 * free)
+    waves = pkg.scene.plan_waves(sizes, budget)
+    DT = pkg.scene.DT
+    res = {"units_b": 0, "ms_b": 0.0, "units_p": 0, "ms_p": 0.0, "units_e": 0, "ms_e": 0.0,
+           "frame_ms": [], "launches": 0, "h2d": 0, "d2h": 0, "truncations": 0, "overflows": 0}
+    clocks = ClockSampler(0)
+    clocks.start()
+    for wave in waves:
+        scs = [built[i][0] for i in wave]
+        fs = [pkg.SCPHDCameraCalibration(built[i][1]) for i in wave]
+        dfr = [[torch.tensor(np.ascontiguousarray(z.T), dtype=torch.float64, device=dev) for z in sc.frames]
+               for sc in scs]
+        torch.cuda.synchronize()
+        batch = pkg.SCPHDBatch(fs, use_graph=True)
+        stream = torch.cuda.ExternalStream(batch.stream_handle())
+        k = 0
+
+        def bstep():
+            nonlocal k
+            batch.step_device(DT, [(z[k][0].data_ptr(), z[k][1].data_ptr(), z[k][2].data_ptr(), z[k].shape[1],
+                                    sc.fixed[k]) for z, sc in zip(dfr, scs)])
+            k += 1
+
+        def pstep():
+            # the same frame for every member, stepped plain: one filter at a time
+            nonlocal k
+            for f, z, sc in zip(fs, dfr, scs):
+                f.step_device(DT, z[k][0].data_ptr(), z[k][1].data_ptr(), z[k][2].data_ptr(), z[k].shape[1],
+                              sc.fixed[k])
+            k += 1
+
+        for _ in range(PF + W):
+            bstep()
+        batch.synchronize()
+        l0 = pkg.kernel_launches()
+        lb = 0
+        # batched and plain frames alternate in pairs (a fixed-camera and a moving-camera
+        # frame each), so that both forms are timed on maps of the same size; members
+        # stepped plain run on the batch's stream, one filter after another
+        for i in range(n_pairs):
+            for form in ("b", "p"):
+                c0 = [f.counters() for f in fs]
+                e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+                e[0].record(stream)
+                for j in range(2):
+                    (bstep if form == "b" else pstep)()
+                    e[j + 1].record(stream)
+                e[2].synchronize()
+                c1 = [f.counters() for f in fs]
+                res["ms_" + form] += e[0].elapsed_time(e[2])
+                res["units_" + form] += sum(int(b[6] - a[6]) for a, b in zip(c0, c1))
+                if form == "b":
+                    res["frame_ms"] += [e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])]
+                    res["truncations"] += sum(int(b[0] - a[0]) for a, b in zip(c0, c1))
+                    lb += 12
+        res["launches"] += lb
+        res["overflows"] += sum(int(f.counters()[1]) for f in fs)
+        # end to end: host frames in, parent states out, through the public API
+        c1 = [f.counters() for f in fs]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(K):
+            frames = [(sc.frames[k][:, 0], sc.frames[k][:, 1], sc.frames[k][:, 2], sc.fixed[k]) for sc in scs]
+            batch.step(DT, frames)
+            res["h2d"] += sum(3 * 8 * sc.frames[k].shape[0] for sc in scs)
+            for f in fs:
+                st, lw = f.particles()
+                res["d2h"] += st.nbytes + lw.nbytes
+            k += 1
+        e1.record(stream)
+        e1.synchronize()
+        c2 = [f.counters() for f in fs]
+        res["ms_e"] += e0.elapsed_time(e1)
+        res["units_e"] += sum(int(b[6] - a[6]) for a, b in zip(c1, c2))
+        batch.close()
+        for f in fs:
+            f.close()
+        del dfr
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    clk = clocks.stop()
+    fm = res["frame_ms"]
+    out = {
+        "workload": args.workload, "filters": len(specs), "parents": int(sum(sp["n_parents"] for sp in specs)),
+        "waves": [len(w) for w in waves], "hbm_budget_gb": budget / 1e9,
+        "device_gb": sum(sizes) / 1e9,
+        "batched": {"value": res["units_b"] / (res["ms_b"] / 1e3), "ms_per_step": res["ms_b"] / (2 * n_pairs),
+                    "steps": 2 * n_pairs},
+        "plain": {"value": res["units_p"] / (res["ms_p"] / 1e3), "ms_per_step": res["ms_p"] / (2 * n_pairs)},
+        "batched_over_plain": (res["units_b"] / res["ms_b"]) / (res["units_p"] / res["ms_p"]),
+        "wave_frame_ms": {"p50": float(np.percentile(fm, 50)), "p99": float(np.percentile(fm, 99))},
+        "e2e": {"value": res["units_e"] / (res["ms_e"] / 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": res["h2d"] // K, "d2h_bytes_per_step": res["d2h"] // K},
+        "gpu_launches": int(res["launches"]), "clocks": clk,
+        "counters": {"map_truncations": res["truncations"], "scratch_overflows": res["overflows"]},
+    }
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -386,11 +511,29 @@ def main():
     ap.add_argument("--cpu-frames", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--parents", type=int, default=0, help="override the parent count (profiling only)")
+    ap.add_argument("--filters", type=int, default=64, help="filters of the batched_c2 workload")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload in ("batched_c2", "batched_c0x64"):
+        import torch
+        torch.cuda.set_device(0)
+        pkg = load_package()
+        r = run_batched(args, pkg)
+        K = args.steps
+        line = {"metric": METRIC, "value": r["batched"]["value"], "unit": UNIT, "n_gpus": 1,
+                "steps": r["batched"]["steps"],
+                "warmup": args.warmup, "ms_per_step": r["batched"]["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
+                "config": {"workload": args.workload, "filters": r["filters"], "parents": r["parents"],
+                           "waves": r["waves"], "prefill_frames": args.prefill,
+                           "l2": "no flush: the resident state is larger than L2"},
+                "e2e": r["e2e"], "gpu_launches": r["gpu_launches"], "clocks": r["clocks"],
+                "plain": r["plain"], "batched_over_plain": r["batched_over_plain"],
+                "wave_frame_ms": r["wave_frame_ms"], "counters": r["counters"]}
+        print(json.dumps(line), flush=True)
     else:
         run_b200(args)
 

@@ -223,6 +223,11 @@ scphd_status scphd_merge_components_static(const double* comps, const uint8_t* f
 scphd_status scphd_systematic_resample(const double* weights, int32_t n, double u01,
                                        int32_t* idx);
 
+/* Device memory, in bytes, that scphd_create would allocate for this configuration
+ * (the filter's arena).  Pure arithmetic: needs no device.  For admission by memory
+ * budget; no reference counterpart. */
+scphd_status scphd_device_bytes(const scphd_config* cfg, int64_t* bytes);
+
 /* ------------------------------------------------------------------ batches
  * Many filters advanced together: every batched step runs predict(dt) + update +
  * resample for all member filters with one kernel launch per stage (six per frame,

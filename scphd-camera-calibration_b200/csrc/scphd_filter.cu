@@ -578,6 +578,24 @@ void scphd_config_defaults(scphd_config* c) {
     c->var_d0 = 2; c->var_vu0 = 6; c->var_vv0 = 6; c->var_vd0 = 0.05;
 }
 
+scphd_status scphd_device_bytes(const scphd_config* cfg, int64_t* bytes) {
+    if (!bytes) return fail(SCPHD_ERR_INVALID, "null output");
+    scphd_status s = validate(cfg);
+    if (s != SCPHD_OK) return s;
+    Arena probe;
+    if (cfg->precision == SCPHD_FP64) {
+        Filter<double> f;
+        f.prm = make_params(*cfg);
+        f.carve(probe);
+    } else {
+        Filter<float> f;
+        f.prm = make_params(*cfg);
+        f.carve(probe);
+    }
+    *bytes = (int64_t)probe.used;
+    return SCPHD_OK;
+}
+
 scphd_status scphd_create(const scphd_config* cfg, scphd_filter** out) {
     if (!out) return fail(SCPHD_ERR_INVALID, "null output handle");
     *out = nullptr;
@@ -994,20 +1012,27 @@ struct scphd_batch {
 namespace {
 
 template <typename T> struct Batch final : scphd_batch {
+    // Filters are launched in groups of up to kBatchSlots, each group with its own
+    // parameter table and block maps; six launches per group and frame.
+    struct Group {
+        int first = 0, count = 0;       // filters [first, first + count)
+        SlotTable<T>* tab = nullptr;    // host copy, passed by value at each launch
+        int2* map_parent = nullptr; int n_parent = 0;
+        int2* map_pred = nullptr;   int n_pred = 0;
+        int4* map_lik = nullptr;    int n_lik = 0;
+    };
     int K = 3;
     bool use_graph = false;
     bool captured = false;
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t done = nullptr;
-    Slot<T>* h_slots = nullptr;   // pinned
-    Slot<T>* d_slots = nullptr;
+    std::vector<Group> groups;
+    FrameArgs* h_fa = nullptr;    // pinned, one per filter
+    FrameArgs* d_fa = nullptr;
     double* h_stage = nullptr;    // pinned, 3 x Mcap per filter
     double* d_stage = nullptr;
     std::vector<size_t> stage_off;
     size_t stage_total = 0;
-    int2* d_map_parent = nullptr; int n_parent_ctas = 0;
-    int2* d_map_pred = nullptr;   int n_pred_ctas = 0;
-    int4* d_map_lik = nullptr;    int n_lik_ctas = 0;
     size_t merge_smem = 0;
     void* dev_mem = nullptr;
 
@@ -1015,9 +1040,10 @@ template <typename T> struct Batch final : scphd_batch {
         if (stream) cudaStreamSynchronize(stream);
         if (exec) cudaGraphExecDestroy(exec);
         if (done) cudaEventDestroy(done);
-        if (h_slots) cudaFreeHost(h_slots);
+        if (h_fa) cudaFreeHost(h_fa);
         if (h_stage) cudaFreeHost(h_stage);
         if (dev_mem) cudaFree(dev_mem);
+        for (Group& g : groups) delete g.tab;
         for (scphd_filter* f : fs) {   // give the filters their own streams back
             f->stream = f->own_stream;
             f->own_stream = nullptr;
@@ -1034,43 +1060,60 @@ template <typename T> struct Batch final : scphd_batch {
         K = fs[0]->prm.K;
         CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         CUDA_TRY(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
-        // block maps
-        std::vector<int2> mp, mpred;
-        std::vector<int4> ml;
+        std::vector<std::vector<int2>> mp, mpred;
+        std::vector<std::vector<int4>> ml;
         stage_off.resize(F);
-        for (int f = 0; f < F; ++f) {
-            const Params& pr = fs[f]->prm;
-            for (int q = 0; q < pr.N; ++q) mp.push_back(make_int2(f, q));
-            for (int q = 0; q < pr.N; q += 256) mpred.push_back(make_int2(f, q));
-            const int mb = (pr.Mcap + 127) / 128;
-            for (int q = 0; q < pr.N; ++q)
-                for (int k = 0; k < mb; ++k) ml.push_back(make_int4(f, q, k, 0));
-            stage_off[f] = stage_total;
-            stage_total += 3 * (size_t)pr.Mcap;
-            merge_smem = std::max(merge_smem, merge_smem_bytes<T>(pr.Scap, pr.Gcap, 4));
+        for (int first = 0; first < F; first += kBatchSlots) {
+            Group g;
+            g.first = first;
+            g.count = std::min(kBatchSlots, F - first);
+            g.tab = new SlotTable<T>();
+            mp.emplace_back();
+            mpred.emplace_back();
+            ml.emplace_back();
+            for (int i = 0; i < g.count; ++i) {
+                const Filter<T>* fl = filt(first + i);
+                const Params& pr = fl->prm;
+                g.tab->prm[i] = pr;
+                g.tab->b[i] = fl->b;
+                for (int q = 0; q < pr.N; ++q) mp.back().push_back(make_int2(i, q));
+                for (int q = 0; q < pr.N; q += 256) mpred.back().push_back(make_int2(i, q));
+                const int mb = (pr.Mcap + 127) / 128;
+                for (int q = 0; q < pr.N; ++q)
+                    for (int k = 0; k < mb; ++k) ml.back().push_back(make_int4(i, q, k, 0));
+                stage_off[first + i] = stage_total;
+                stage_total += 3 * (size_t)pr.Mcap;
+                merge_smem = std::max(merge_smem, merge_smem_bytes<T>(pr.Scap, pr.Gcap, 4));
+            }
+            g.n_parent = (int)mp.back().size();
+            g.n_pred = (int)mpred.back().size();
+            g.n_lik = (int)ml.back().size();
+            groups.push_back(g);
         }
-        n_parent_ctas = (int)mp.size();
-        n_pred_ctas = (int)mpred.size();
-        n_lik_ctas = (int)ml.size();
         Arena probe;
-        probe.take<Slot<T>>(F);
+        probe.take<FrameArgs>(F);
         probe.take<double>(stage_total);
-        probe.take<int2>(mp.size());
-        probe.take<int2>(mpred.size());
-        probe.take<int4>(ml.size());
+        for (size_t gi = 0; gi < groups.size(); ++gi) {
+            probe.take<int2>(mp[gi].size());
+            probe.take<int2>(mpred[gi].size());
+            probe.take<int4>(ml[gi].size());
+        }
         CUDA_TRY(cudaMalloc(&dev_mem, probe.used));
         Arena a;
         a.base = static_cast<char*>(dev_mem);
-        d_slots = a.take<Slot<T>>(F);
+        d_fa = a.take<FrameArgs>(F);
         d_stage = a.take<double>(stage_total);
-        d_map_parent = a.take<int2>(mp.size());
-        d_map_pred = a.take<int2>(mpred.size());
-        d_map_lik = a.take<int4>(ml.size());
-        CUDA_TRY(cudaMallocHost(&h_slots, sizeof(Slot<T>) * F));
+        for (size_t gi = 0; gi < groups.size(); ++gi) {
+            Group& g = groups[gi];
+            g.map_parent = a.take<int2>(mp[gi].size());
+            g.map_pred = a.take<int2>(mpred[gi].size());
+            g.map_lik = a.take<int4>(ml[gi].size());
+            CUDA_TRY(cudaMemcpy(g.map_parent, mp[gi].data(), sizeof(int2) * mp[gi].size(), cudaMemcpyHostToDevice));
+            CUDA_TRY(cudaMemcpy(g.map_pred, mpred[gi].data(), sizeof(int2) * mpred[gi].size(), cudaMemcpyHostToDevice));
+            CUDA_TRY(cudaMemcpy(g.map_lik, ml[gi].data(), sizeof(int4) * ml[gi].size(), cudaMemcpyHostToDevice));
+        }
+        CUDA_TRY(cudaMallocHost(&h_fa, sizeof(FrameArgs) * F));
         CUDA_TRY(cudaMallocHost(&h_stage, sizeof(double) * std::max<size_t>(stage_total, 1)));
-        CUDA_TRY(cudaMemcpy(d_map_parent, mp.data(), sizeof(int2) * mp.size(), cudaMemcpyHostToDevice));
-        CUDA_TRY(cudaMemcpy(d_map_pred, mpred.data(), sizeof(int2) * mpred.size(), cudaMemcpyHostToDevice));
-        CUDA_TRY(cudaMemcpy(d_map_lik, ml.data(), sizeof(int4) * ml.size(), cudaMemcpyHostToDevice));
         if (merge_smem > 227 * 1024) return fail(SCPHD_ERR_CAPACITY, "batch merge needs more than 227 KB of shared memory");
         if (K == 2) {
             CUDA_TRY(allow_dynamic_smem((const void*)k_merge_batch<T, 2>));
@@ -1087,26 +1130,40 @@ template <typename T> struct Batch final : scphd_batch {
         return SCPHD_OK;
     }
 
+    // kernels of one frame, stage by stage over the groups
     template <int KK> scphd_status launch_all() {
-        const int F = (int)fs.size();
-        k_predict_parents_batch<T><<<n_pred_ctas, 256, 0, stream>>>(d_slots, d_map_pred);
-        LAUNCHED();
-        k_cloud_fit_batch<T, KK><<<n_parent_ctas, 256, 0, stream>>>(d_slots, d_map_parent);
-        LAUNCHED();
-        k_likelihood_batch<T, KK><<<n_lik_ctas, 128, 0, stream>>>(d_slots, d_map_lik);
-        LAUNCHED();
-        k_merge_batch<T, KK><<<n_parent_ctas, 128, merge_smem, stream>>>(d_slots, d_map_parent);
-        LAUNCHED();
-        k_weights_batch<T><<<F, 1024, 0, stream>>>(d_slots);
-        LAUNCHED();
-        k_resample_batch<T><<<F, 1024, 0, stream>>>(d_slots);
-        LAUNCHED();
+        for (const Group& g : groups) {
+            k_predict_parents_batch<T><<<g.n_pred, 256, 0, stream>>>(*g.tab, d_fa + g.first, g.map_pred);
+            LAUNCHED();
+        }
+        for (const Group& g : groups) {
+            k_cloud_fit_batch<T, KK><<<g.n_parent, 256, 0, stream>>>(*g.tab, d_fa + g.first, g.map_parent);
+            LAUNCHED();
+        }
+        for (const Group& g : groups) {
+            k_likelihood_batch<T, KK><<<g.n_lik, 128, 0, stream>>>(*g.tab, d_fa + g.first, g.map_lik);
+            LAUNCHED();
+        }
+        for (const Group& g : groups) {
+            k_merge_batch<T, KK><<<g.n_parent, 128, merge_smem, stream>>>(*g.tab, d_fa + g.first, g.map_parent);
+            LAUNCHED();
+        }
+        for (const Group& g : groups) {
+            k_weights_batch<T><<<g.count, 1024, 0, stream>>>(*g.tab, d_fa + g.first);
+            LAUNCHED();
+        }
+        for (const Group& g : groups) {
+            k_resample_batch<T><<<g.count, 1024, 0, stream>>>(*g.tab, d_fa + g.first);
+            LAUNCHED();
+        }
         return SCPHD_OK;
     }
 
+    int launches_per_frame() const { return 6 * (int)groups.size(); }
+
     scphd_status enqueue() {
         CUDA_TRY(cudaMemcpyAsync(d_stage, h_stage, sizeof(double) * stage_total, cudaMemcpyHostToDevice, stream));
-        CUDA_TRY(cudaMemcpyAsync(d_slots, h_slots, sizeof(Slot<T>) * fs.size(), cudaMemcpyHostToDevice, stream));
+        CUDA_TRY(cudaMemcpyAsync(d_fa, h_fa, sizeof(FrameArgs) * fs.size(), cudaMemcpyHostToDevice, stream));
         return K == 2 ? launch_all<2>() : launch_all<3>();
     }
 
@@ -1135,10 +1192,7 @@ template <typename T> struct Batch final : scphd_batch {
             const scphd_frame& fr = frames[f];
             fl->frame++;
             if (fl->frame >= (1u << 20)) return fail(SCPHD_ERR_CAPACITY, "frame counter exhausted (2^20 frames)");
-            Slot<T>& sl = h_slots[f];
-            sl.prm = fl->prm;
-            sl.b = fl->b;
-            FrameArgs& fa = sl.fa;
+            FrameArgs& fa = h_fa[f];
             fa.cur = fl->cur;
             fa.M = fr.n;
             fa.fixed = fr.fixed_camera ? 1 : 0;
@@ -1176,10 +1230,11 @@ template <typename T> struct Batch final : scphd_batch {
                 cudaGraphDestroy(g);
                 if (e != cudaSuccess) return fail(SCPHD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
                 captured = true;
-                g_launches.fetch_sub(6, std::memory_order_relaxed);   // captured, not run: counted at replay
+                // captured, not run: counted at replay
+                g_launches.fetch_sub(launches_per_frame(), std::memory_order_relaxed);
             }
             CUDA_TRY(cudaGraphLaunch(exec, stream));
-            g_launches.fetch_add(6, std::memory_order_relaxed);
+            g_launches.fetch_add(launches_per_frame(), std::memory_order_relaxed);
         } else {
             scphd_status s = enqueue();
             if (s != SCPHD_OK) return s;

@@ -72,11 +72,14 @@ struct FrameArgs {
     const double* zd;
 };
 
-// One filter of a batch: its constants, buffers and frame arguments.
-template <typename T> struct Slot {
-    Params prm;
-    Bufs<T> b;
-    FrameArgs fa;
+// Up to kBatchSlots filters of a batch per launch: their constants and buffers as
+// one kernel parameter (read-only parameter space, like a single filter's Params;
+// 32 x 744 bytes fits the 32 KB parameter limit).  Each frame's per-filter
+// arguments are a separate FrameArgs array in global memory.
+constexpr int kBatchSlots = 32;
+template <typename T> struct SlotTable {
+    Params prm[kBatchSlots];
+    Bufs<T> b[kBatchSlots];
 };
 
 __device__ __forceinline__ uint32_t tie_key(uint32_t r) {
@@ -381,12 +384,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
 }
 
 template <typename T, int K>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_cloud_fit_batch(const Slot<T>* slots, const int2* map) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
+    k_cloud_fit_batch(const __grid_constant__ SlotTable<T> tab, const FrameArgs* fas, const int2* map) {
     const int2 fp = map[blockIdx.x];
-    const Slot<T>& sl = slots[fp.x];
-    const FrameArgs& fa = sl.fa;
-    cloud_fit_body<T, K>(sl.prm, sl.b, fa.cur, fa.M, fa.fixed, fa.has_pred, fa.dt, fa.pred_frame, fa.sample_frame,
-                         fa.zu, fa.zv, fa.zd, fp.y);
+    const FrameArgs fa = fas[fp.x];
+    cloud_fit_body<T, K>(tab.prm[fp.x], tab.b[fp.x], fa.cur, fa.M, fa.fixed, fa.has_pred, fa.dt, fa.pred_frame,
+                         fa.sample_frame, fa.zu, fa.zv, fa.zd, fp.y);
 }
 
 // ---------------------------------------------------------------- (c) likelihood
@@ -516,11 +519,12 @@ __global__ void __launch_bounds__(128) k_likelihood(__grid_constant__ const Para
 
 // map entry: (filter, parent, measurement block); blocks past a filter's M exit
 template <typename T, int K>
-__global__ void __launch_bounds__(128) k_likelihood_batch(const Slot<T>* slots, const int4* map) {
+__global__ void __launch_bounds__(128)
+    k_likelihood_batch(const __grid_constant__ SlotTable<T> tab, const FrameArgs* fas, const int4* map) {
     const int4 e = map[blockIdx.x];
-    const Slot<T>& sl = slots[e.x];
-    if (e.z * (int)blockDim.x >= sl.fa.M) return;
-    likelihood_body<T, K>(sl.prm, sl.b, sl.fa.cur, sl.fa.M, e.y, e.z);
+    const int M = fas[e.x].M;
+    if (e.z * (int)blockDim.x >= M) return;
+    likelihood_body<T, K>(tab.prm[e.x], tab.b[e.x], fas[e.x].cur, M, e.y, e.z);
 }
 
 // ---------------------------------------------------------------- (d) merge
@@ -1259,10 +1263,11 @@ __global__ void __launch_bounds__(128) k_merge(__grid_constant__ const Params pr
 }
 
 template <typename T, int K>
-__global__ void __launch_bounds__(128) k_merge_batch(const Slot<T>* slots, const int2* map) {
+__global__ void __launch_bounds__(128)
+    k_merge_batch(const __grid_constant__ SlotTable<T> tab, const FrameArgs* fas, const int2* map) {
     const int2 fp = map[blockIdx.x];
-    const Slot<T>& sl = slots[fp.x];
-    merge_body<T, K>(sl.prm, sl.b, sl.fa.cur, sl.fa.M, sl.fa.fixed, fp.y);
+    const FrameArgs fa = fas[fp.x];
+    merge_body<T, K>(tab.prm[fp.x], tab.b[fp.x], fa.cur, fa.M, fa.fixed, fp.y);
 }
 
 // ---------------------------------------------------------------- parent weights
@@ -1320,9 +1325,10 @@ __global__ void __launch_bounds__(1024) k_weights(int N, double* lw, const doubl
 }
 
 template <typename T>
-__global__ void __launch_bounds__(1024) k_weights_batch(const Slot<T>* slots) {
-    const Slot<T>& sl = slots[blockIdx.x];
-    weights_body(sl.prm.N, sl.b.lw, sl.b.loglik, sl.fa.fixed ? 0 : 1, sl.b.scal, sl.b.counters);
+__global__ void __launch_bounds__(1024) k_weights_batch(const __grid_constant__ SlotTable<T> tab, const FrameArgs* fas) {
+    const int f = blockIdx.x;
+    const Bufs<T>& b = tab.b[f];
+    weights_body(tab.prm[f].N, b.lw, b.loglik, fas[f].fixed ? 0 : 1, b.scal, b.counters);
 }
 
 // ---------------------------------------------------------------- (e) resample
@@ -1434,23 +1440,23 @@ __global__ void __launch_bounds__(1024) k_resample(__grid_constant__ const Param
 }
 
 template <typename T>
-__global__ void __launch_bounds__(1024) k_resample_batch(const Slot<T>* slots) {
-    const Slot<T>& sl = slots[blockIdx.x];
-    const Bufs<T>& b = sl.b;
-    resample_body(sl.prm, b.lw, b.ext, b.ext_tmp, b.src, b.src_tmp, b.cum, b.scal, b.flags, b.resample_idx,
-                  sl.fa.frame, 0, -1.0, b.counters);
+__global__ void __launch_bounds__(1024) k_resample_batch(const __grid_constant__ SlotTable<T> tab, const FrameArgs* fas) {
+    const int f = blockIdx.x;
+    const Bufs<T>& b = tab.b[f];
+    resample_body(tab.prm[f], b.lw, b.ext, b.ext_tmp, b.src, b.src_tmp, b.cum, b.scal, b.flags, b.resample_idx,
+                  fas[f].frame, 0, -1.0, b.counters);
 }
 
 // map entry: (filter, first parent of a 256-parent block)
 template <typename T>
-__global__ void k_predict_parents_batch(const Slot<T>* slots, const int2* map) {
+__global__ void k_predict_parents_batch(const __grid_constant__ SlotTable<T> tab, const FrameArgs* fas, const int2* map) {
     const int2 fp = map[blockIdx.x];
-    const Slot<T>& sl = slots[fp.x];
+    const Bufs<T>& b = tab.b[fp.x];
     if (fp.y == 0 && threadIdx.x == 0) {   // counters of "the last update" start at 0
-        sl.b.counters[4] = 0;
-        sl.b.counters[5] = 0;
+        b.counters[4] = 0;
+        b.counters[5] = 0;
     }
-    predict_parents_body(sl.prm, sl.b.ext, sl.fa.dt, sl.fa.frame, fp.y + threadIdx.x);
+    predict_parents_body(tab.prm[fp.x], b.ext, fas[fp.x].dt, fas[fp.x].frame, fp.y + threadIdx.x);
 }
 
 // ---------------------------------------------------------------- cloud materialisation

@@ -187,3 +187,47 @@ def workload(name: str, precision: int = 0, filter_index: int = 0, n_frames: Opt
                         calib=sc.calib, seed=sd)
     cfg.max_survivors = w["max_survivors"]
     return sc, cfg
+
+
+# ------------------------------------------------------------------ many filters
+def batched_specs(n_filters: int = 64, seed: int = SCENE_SEED_BASE + 2000):
+    """Filters of the many-filter workload: parent counts log-uniform in [512, 8192],
+    landmark counts uniform in [20, 400], clutter rates uniform in [5, 80], each with
+    its own seeded scene and trajectory."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n_filters):
+        n = int(round(float(np.exp(rng.uniform(np.log(512.0), np.log(8192.0))))))
+        specs.append(dict(index=i, n_parents=n, n_landmarks=int(rng.integers(20, 401)),
+                          clutter=float(rng.uniform(5.0, 80.0))))
+    return specs
+
+
+def spec_filter(spec: dict, n_frames: int, precision: int = 0, max_gaussians: int = 256, config_index: int = 2,
+                survivors_per_gaussian: int = 3):
+    """(scene, config) of one filter of a many-filter workload.  The measurement
+    capacity is the scene's largest frame rounded up to 32."""
+    sd = scene_seed(config_index, spec["index"])
+    sc = make_scene(spec["n_landmarks"], n_frames, spec["clutter"], sd)
+    mmax = max(int(z.shape[0]) for z in sc.frames) if sc.frames else 0
+    mcap = max(32, (mmax + 8 + 31) // 32 * 32)
+    cfg = filter_config(spec["n_parents"], max_gaussians, mcap, spec["clutter"], precision, calib=sc.calib, seed=sd)
+    cfg.max_survivors = survivors_per_gaussian * max_gaussians
+    return sc, cfg
+
+
+def plan_waves(sizes, budget: int):
+    """Greedy grouping of filters (in order) into device-resident waves whose summed
+    device bytes stay within budget; a filter larger than the budget is refused."""
+    waves, cur, used = [], [], 0
+    for i, b in enumerate(sizes):
+        if b > budget:
+            raise ValueError(f"filter {i} needs {b} bytes, more than the budget {budget}")
+        if used + b > budget and cur:
+            waves.append(cur)
+            cur, used = [], 0
+        cur.append(i)
+        used += b
+    if cur:
+        waves.append(cur)
+    return waves

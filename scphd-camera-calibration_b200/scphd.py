@@ -172,6 +172,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "scphd_stream": (vp, [vp]),
         "scphd_set_profiling": (i32, [vp, i32]),
         "scphd_get_stage_times": (i32, [vp, P(d), P(i64)]),
+        "scphd_device_bytes": (i32, [P(ScphdConfig), P(i64)]),
         "scphd_batch_create": (i32, [P(vp), i32, i32, P(vp)]),
         "scphd_batch_destroy": (i32, [vp]),
         "scphd_batch_step": (i32, [vp, d, P(ScphdFrame)]),
@@ -208,6 +209,14 @@ def _iptr(a: Optional[np.ndarray]):
 
 def _f64(x) -> np.ndarray:
     return np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+
+
+def device_bytes(config: ScphdConfig) -> int:
+    """Device memory a filter with this configuration allocates (no device needed)."""
+    lib = load_library()
+    out = ctypes.c_int64(0)
+    _check(lib.scphd_device_bytes(ctypes.byref(config), ctypes.byref(out)))
+    return int(out.value)
 
 
 def kernel_launches() -> int:
