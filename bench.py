@@ -498,6 +498,97 @@ def run_batched(args, pkg, quiet=False):
     return out
 
 
+def run_serving(args, pkg):
+    """Serving workload: Poisson arrivals (20 jobs/s for --serve-seconds) of
+    calibration jobs of uneven size, admitted first come, first served by the
+    server under an 80% HBM budget and advanced in batched steps.  Scenes are
+    generated when a job is handed to the server (host memory stays bounded while
+    the offered load exceeds what the device serves); a job's wait counts from its
+    arrival time.  Reports updates/s over the serving window (wall clock), per
+    job-frame latency (device time of the step that advanced it), admission waits."""
+    import torch
+    prec = pkg.SCPHD_FP32 if args.precision == "fp32" else pkg.SCPHD_FP64
+    arrivals = pkg.scene.serving_arrivals(seconds=args.serve_seconds)
+    free, total = torch.cuda.mem_get_info(torch.device("cuda", 0))
+    budget = int(0.8 * free)
+    srv = pkg.SCPHDServer(budget, precision=prec, meas_dim=3, use_graph=True)
+    DT = pkg.scene.DT
+    # the clients: a producer thread turns arrivals into job data, in arrival order
+    import queue as _queue
+    import threading
+    ready = _queue.Queue(maxsize=4)
+    stop = threading.Event()
+
+    def produce():
+        for ta, sp in arrivals:
+            sc, cfg = pkg.scene.spec_filter(sp, sp["n_frames"], prec, config_index=4)
+            while not stop.is_set():
+                try:
+                    ready.put((ta, sc, cfg), timeout=0.1)
+                    break
+                except _queue.Full:
+                    pass
+            if stop.is_set():
+                return
+
+    producer = threading.Thread(target=produce, daemon=True)
+    producer.start()
+    held = None
+    submitted, admitted_at, arrival_of = [], {}, {}
+    clocks = ClockSampler(0)
+    clocks.start()
+    t0 = time.perf_counter()
+    while True:
+        now = time.perf_counter() - t0
+        if now >= args.serve_seconds:
+            break
+        # hand arrived jobs to the server while its own queue is short
+        while len(submitted) - len(admitted_at) < 2:
+            if held is None:
+                try:
+                    held = ready.get_nowait()
+                except _queue.Empty:
+                    break
+            if held[0] > now:
+                break
+            ta, sc, cfg = held
+            jid = srv.submit(cfg, sc.frames, sc.fixed, DT)
+            submitted.append(jid)
+            arrival_of[jid] = ta
+            held = None
+        for jid in submitted:
+            if jid not in admitted_at and srv.status(jid)[0] != pkg.JOB_QUEUED:
+                admitted_at[jid] = time.perf_counter() - t0
+        if srv.step() == 0:
+            time.sleep(0.001)
+    stop.set()
+    srv.drain()
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    st = srv.stats()
+    ms, nj = srv.step_times()
+    lat = np.repeat(ms, nj) if len(ms) else np.zeros(1)
+    waits = [admitted_at[j] - arrival_of[j] for j in admitted_at]
+    srv.close()
+    line = {
+        "metric": METRIC, "value": st["units"] / wall, "unit": UNIT, "n_gpus": 1, "steps": int(st["steps"]),
+        "warmup": 0, "ms_per_step": float(np.mean(ms)) if len(ms) else None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
+        "config": {"workload": "serving_c4", "arrival_rate_per_s": 20.0, "window_s": args.serve_seconds,
+                   "arrived": sum(1 for t, _ in arrivals if t <= wall), "handed_to_server": len(submitted),
+                   "admitted": len(admitted_at), "completed": st["done"], "hbm_budget_gb": budget / 1e9,
+                   "note": "value = updates over the wall-clock serving window, starting from an empty server"},
+        "frame_latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                             "max": float(lat.max())},
+        "admission_wait_s": {"p50": float(np.percentile(waits, 50)) if waits else None,
+                             "p99": float(np.percentile(waits, 99)) if waits else None},
+        "device_busy_fraction": float(ms.sum() / 1e3 / wall) if len(ms) else 0.0,
+        "job_frames": int(st["job_frames"]), "batch_rebuilds": int(st["rebuilds"]),
+        "mean_jobs_per_step": float(nj.mean()) if len(nj) else 0.0, "clocks": clk,
+    }
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -512,11 +603,16 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--parents", type=int, default=0, help="override the parent count (profiling only)")
     ap.add_argument("--filters", type=int, default=64, help="filters of the batched_c2 workload")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="serving window of serving_c4")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "serving_c4":
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(run_serving(args, load_package())), flush=True)
     elif args.workload in ("batched_c2", "batched_c0x64"):
         import torch
         torch.cuda.set_device(0)

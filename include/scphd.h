@@ -261,6 +261,50 @@ scphd_status scphd_batch_step_device(scphd_batch* b, double dt, const scphd_fram
 /* The batch's CUDA stream (a cudaStream_t). */
 void* scphd_batch_stream(scphd_batch* b);
 
+/* ------------------------------------------------------------------ serving
+ * A resident request loop over batches.  A job is a filter configuration plus its
+ * whole frame sequence.  Jobs may be submitted at any time; they are admitted first
+ * come, first served while their device memory (filter arena + frame sequence) fits
+ * the server's budget, kept resident between frames, and advanced together: each
+ * scphd_server_step steps every resident job by one frame in one batched step.  A
+ * job that has processed its last frame is retired at the next call: its parent
+ * states and log-weights are copied out, its memory returns to the budget, and
+ * queued jobs that now fit are admitted.  Each job's result equals that of the same
+ * filter stepped alone.  All jobs of a server share device, precision, meas_dim and dt.
+ * Calls on one server must be serialised by the caller.  No reference counterpart
+ * (the reference runs one filter per process). */
+typedef struct scphd_server scphd_server;
+enum { SCPHD_JOB_QUEUED = 0, SCPHD_JOB_RUNNING = 1, SCPHD_JOB_DONE = 2 };
+
+scphd_status scphd_server_create(int32_t device, int32_t precision, int32_t meas_dim, int64_t budget_bytes,
+                                 int32_t use_graph, scphd_server** out);
+scphd_status scphd_server_destroy(scphd_server* s);
+/* Frame k has sizes[k] measurements at offset sizes[0] + ... + sizes[k-1] of u, v and
+ * d (d NULL when meas_dim == 2); fixed[k] != 0 marks a fixed-camera frame; every
+ * frame is preceded by predict(dt).  Host arrays, copied during the call.  A job
+ * larger than the whole budget is refused with SCPHD_ERR_CAPACITY. */
+scphd_status scphd_server_submit(scphd_server* s, const scphd_config* cfg, int32_t n_frames, const int32_t* sizes,
+                                 const double* u, const double* v, const double* d, const int32_t* fixed,
+                                 double dt, int64_t* job_id);
+/* One serving iteration: wait for the previous step, retire the jobs it finished,
+ * admit queued jobs that fit, then queue one batched step of every resident job and
+ * return without waiting for it.  *stepped = jobs in that step (0: nothing resident). */
+scphd_status scphd_server_step(scphd_server* s, int32_t* stepped);
+/* Wait for the last step and retire the jobs it finished. */
+scphd_status scphd_server_drain(scphd_server* s);
+scphd_status scphd_server_job_status(scphd_server* s, int64_t job, int32_t* state, int32_t* frames_done);
+/* Result of a DONE job: states (n_parents x 12, row-major) and log-weights (n_parents). */
+scphd_status scphd_server_job_result(scphd_server* s, int64_t job, double* states, double* log_weights);
+/* out[0] queued jobs, [1] running, [2] done, [3] device bytes in use, [4] steps,
+ * [5] job-frames stepped, [6] Gaussian-measurement updates of all admitted jobs
+ * (reading the running jobs' counters waits for their queued work), [7] batch
+ * rebuilds. */
+scphd_status scphd_server_stats(scphd_server* s, int64_t out[8]);
+/* Device time in ms of completed steps first .. first+max-1 (oldest first) and the
+ * number of jobs each advanced; *n_out = entries written. */
+scphd_status scphd_server_step_times(scphd_server* s, int64_t first, int32_t max, double* ms, int32_t* jobs,
+                                     int32_t* n_out);
+
 /* Text of the last error on this thread. */
 const char* scphd_last_error(void);
 

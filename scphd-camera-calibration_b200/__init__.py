@@ -5,6 +5,6 @@ the repository root helpers (bench.py, __graft_entry__.py, tests/conftest.py),
 which registers it as the module `scphd_b200`.
 """
 from .scphd import (SCPHD_FP32, SCPHD_FP64, SCPHD_MIX_FITTED, SCPHD_MIX_MERGED,  # noqa: F401
-                    SCPHDBatch, SCPHDCameraCalibration, ScphdConfig, ScphdError, ScphdFrame, kernel_launches,
+                    JOB_DONE, JOB_QUEUED, JOB_RUNNING, SCPHDBatch, SCPHDCameraCalibration, SCPHDServer, ScphdConfig, ScphdError, ScphdFrame, kernel_launches,
                     device_bytes, load_library, merge_components, reference_defaults, systematic_resample)
 from . import evaluate, scene  # noqa: F401

@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(CSRC, "libscphd_b200.so")
-SOURCES = ["scphd_filter.cu"]
+SOURCES = ["scphd_filter.cu", "scphd_server.cu"]
 DEPS = SOURCES + ["scphd_kernels.cuh", "scphd_device.cuh"]
 
 NVCC_FLAGS = [

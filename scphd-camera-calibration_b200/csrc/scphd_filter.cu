@@ -71,6 +71,11 @@ struct Arena {
 
 }  // namespace
 
+// error text for the other translation units of the library (not exported)
+__attribute__((visibility("hidden"))) scphd_status scphd_fail_internal(scphd_status st, const char* msg) {
+    return fail(st, msg);
+}
+
 struct scphd_filter {
     scphd_config cfg;
     Params prm;

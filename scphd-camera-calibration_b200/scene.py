@@ -231,3 +231,18 @@ def plan_waves(sizes, budget: int):
     if cur:
         waves.append(cur)
     return waves
+
+
+def serving_arrivals(rate: float = 20.0, seconds: float = 60.0, seed: int = SCENE_SEED_BASE + 4000):
+    """Poisson arrivals of calibration jobs: (time, spec) with 100-1000 frames
+    (uniform), 512-8192 parents (log-uniform), 20-400 landmarks, clutter 5-80."""
+    rng = np.random.default_rng(seed)
+    t, out, i = 0.0, [], 0
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t >= seconds:
+            return out
+        out.append((t, dict(index=i, n_parents=int(round(float(np.exp(rng.uniform(np.log(512.0), np.log(8192.0)))))),
+                            n_landmarks=int(rng.integers(20, 401)), clutter=float(rng.uniform(5.0, 80.0)),
+                            n_frames=int(rng.integers(100, 1001)))))
+        i += 1

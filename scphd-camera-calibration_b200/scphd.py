@@ -178,6 +178,15 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "scphd_batch_step": (i32, [vp, d, P(ScphdFrame)]),
         "scphd_batch_step_device": (i32, [vp, d, P(ScphdFrame)]),
         "scphd_batch_stream": (vp, [vp]),
+        "scphd_server_create": (i32, [i32, i32, i32, i64, i32, P(vp)]),
+        "scphd_server_destroy": (i32, [vp]),
+        "scphd_server_submit": (i32, [vp, P(ScphdConfig), i32, P(i32), P(d), P(d), P(d), P(i32), d, P(i64)]),
+        "scphd_server_step": (i32, [vp, P(i32)]),
+        "scphd_server_drain": (i32, [vp]),
+        "scphd_server_job_status": (i32, [vp, i64, P(i32), P(i32)]),
+        "scphd_server_job_result": (i32, [vp, i64, P(d), P(d)]),
+        "scphd_server_stats": (i32, [vp, P(i64)]),
+        "scphd_server_step_times": (i32, [vp, i64, i32, P(d), P(i32), P(i32)]),
         "scphd_last_error": (ctypes.c_char_p, []),
         "scphd_kernel_launches": (i64, []),
     }
@@ -446,6 +455,91 @@ class SCPHDBatch:
     def synchronize(self) -> None:
         for f in self.filters:
             f.synchronize()
+
+
+JOB_QUEUED, JOB_RUNNING, JOB_DONE = 0, 1, 2
+
+
+class SCPHDServer:
+    """Resident serving loop (scphd_server_* in include/scphd.h): jobs are admitted
+    first come, first served under a device-memory budget and advanced together, one
+    batched frame per step()."""
+
+    def __init__(self, budget_bytes: int, precision: int = 0, meas_dim: int = 3, device: int = 0,
+                 use_graph: bool = True):
+        self._lib = load_library()
+        self.precision, self.meas_dim, self.device = precision, meas_dim, device
+        h = ctypes.c_void_p()
+        _check(self._lib.scphd_server_create(int(device), int(precision), int(meas_dim), int(budget_bytes),
+                                             int(bool(use_graph)), ctypes.byref(h)))
+        self._h = h
+        self._parents = {}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            _check(self._lib.scphd_server_destroy(self._h))
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, config: ScphdConfig, frames, fixed, dt: float) -> int:
+        """frames: list of (n, meas_dim) arrays (u, v[, d]); fixed: per-frame flags."""
+        sizes = np.array([len(z) for z in frames], np.int32)
+        parts = [np.asarray(z, np.float64).reshape(len(z), -1)[:, :self.meas_dim] for z in frames if len(z)]
+        cat = np.concatenate(parts, axis=0) if parts else np.zeros((0, self.meas_dim))
+        u, v = _f64(cat[:, 0]), _f64(cat[:, 1])
+        d = _f64(cat[:, 2]) if self.meas_dim == 3 else None
+        fx = np.asarray(fixed, np.int32)
+        jid = ctypes.c_int64(0)
+        cfg = config.copy()
+        _check(self._lib.scphd_server_submit(self._h, ctypes.byref(cfg), int(len(frames)), _iptr(sizes), _dptr(u),
+                                             _dptr(v), _dptr(d), _iptr(fx), float(dt), ctypes.byref(jid)))
+        self._parents[jid.value] = int(cfg.n_parents)
+        return int(jid.value)
+
+    def step(self) -> int:
+        n = ctypes.c_int32(0)
+        _check(self._lib.scphd_server_step(self._h, ctypes.byref(n)))
+        return int(n.value)
+
+    def drain(self) -> None:
+        _check(self._lib.scphd_server_drain(self._h))
+
+    def status(self, job: int):
+        st, fd = ctypes.c_int32(0), ctypes.c_int32(0)
+        _check(self._lib.scphd_server_job_status(self._h, int(job), ctypes.byref(st), ctypes.byref(fd)))
+        return int(st.value), int(fd.value)
+
+    def result(self, job: int):
+        n = self._parents[job]
+        st = np.zeros((n, 12), np.float64)
+        lw = np.zeros(n, np.float64)
+        _check(self._lib.scphd_server_job_result(self._h, int(job), _dptr(st), _dptr(lw)))
+        return st, lw
+
+    def stats(self) -> dict:
+        out = (ctypes.c_int64 * 8)()
+        _check(self._lib.scphd_server_stats(self._h, out))
+        keys = ("queued", "running", "done", "bytes_in_use", "steps", "job_frames", "units", "rebuilds")
+        return dict(zip(keys, [int(x) for x in out]))
+
+    def step_times(self, first: int = 0, max_n: int = 1 << 20):
+        ms = np.zeros(max_n, np.float64)
+        jobs = np.zeros(max_n, np.int32)
+        n = ctypes.c_int32(0)
+        _check(self._lib.scphd_server_step_times(self._h, int(first), int(max_n), _dptr(ms), _iptr(jobs),
+                                                 ctypes.byref(n)))
+        return ms[:n.value], jobs[:n.value]
 
 
 def merge_components(comps: np.ndarray, flags: np.ndarray, min_separation: float,

@@ -64,3 +64,37 @@ def test_workload_configs(pkg):
     sc, cfg = pkg.scene.workload("plain_c1", n_frames=2)
     assert cfg.n_parents == 4096 and cfg.max_gaussians == 256
     assert cfg.kappa == pytest.approx(50.0 / (640 * 480 * 63))
+
+
+def test_server_without_device_fails_loudly(pkg):
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("device present")
+    except Exception:
+        pass
+    with pytest.raises(pkg.ScphdError) as e:
+        pkg.SCPHDServer(1 << 30)
+    assert e.value.status in (2, 5)
+
+
+def test_device_bytes_and_wave_plan(pkg):
+    """Device footprint is pure arithmetic (no device) and grows with every capacity;
+    the wave planner keeps each wave within the budget and the filters in order."""
+    base = pkg.scene.filter_config(n_parents=100, max_gaussians=64, max_meas=64, clutter_rate=5.0)
+    b0 = pkg.device_bytes(base)
+    for field, val in (("n_parents", 200), ("max_gaussians", 128), ("max_measurements", 256),
+                       ("particles_per_feature", 200), ("precision", 1)):
+        c = base.copy()
+        setattr(c, field, val)
+        assert pkg.device_bytes(c) > b0, field
+    bad = base.copy()
+    bad.meas_dim = 4
+    with pytest.raises(pkg.ScphdError):
+        pkg.device_bytes(bad)
+    sizes = [5, 3, 4, 9, 1, 1, 8]
+    waves = pkg.scene.plan_waves(sizes, 10)
+    assert [i for w in waves for i in w] == list(range(len(sizes)))
+    assert all(sum(sizes[i] for i in w) <= 10 for w in waves)
+    with pytest.raises(ValueError):
+        pkg.scene.plan_waves([11], 10)
