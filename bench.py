@@ -589,6 +589,162 @@ def run_serving(args, pkg):
     return line
 
 
+def _match_rows(A, B, mean_cols, var_cols):
+    """Pair the rows of two mixtures (nearest mean in units of A's standard
+    deviations); returns per-pair |dmean|/sd and relative variance errors."""
+    if not len(A) or not len(B):
+        return np.zeros(0), np.zeros(0)
+    sd = np.sqrt(np.maximum(A[:, var_cols], 1e-30))
+    d = np.abs(B[None, :, mean_cols] - A[:, None, mean_cols]) / sd[:, None, :]
+    j = np.argmin(d.max(axis=2), axis=1)
+    dm = d[np.arange(len(A)), j].ravel()
+    dv = (np.abs(B[j][:, var_cols] - A[:, var_cols]) / np.maximum(np.abs(A[:, var_cols]), 1e-30)).ravel()
+    return dm, dv
+
+
+def _capture_state(f):
+    """Whole filter state as set_state takes it (Euclidean clouds)."""
+    st, lw = f.particles()
+    sizes = f.map_sizes()
+    ws, cl, om = [], [], []
+    for p in range(f.n_parents):
+        if sizes[p]:
+            ws.append(f.map_weights(p))
+            x, o = f.map_clouds(p)
+            cl.append(x)
+            om.append(o)
+    cat = lambda xs, shp: np.concatenate(xs) if xs else np.zeros(shp)
+    P = int(f.config.particles_per_feature)
+    return st, lw, sizes, cat(ws, (0,)), cat(cl, (0, 6, P)), cat(om, (0, P))
+
+
+def run_precision(args, pkg):
+    """Precision study on precision_c3 (16384 parents, 400 landmarks, <= 512
+    Gaussians, clutter 100, 300 frames).  FP32 mode computes the Kalman algebra,
+    refits and merge in FP32; parent states, the log-weight accumulation and the
+    resampling prefix sum stay FP64 in both modes.
+
+    (1) One-step errors: a 256-parent FP64 filter on the same scene is run; at
+    checkpoint frames its whole state is loaded (set_state) into a fresh FP64 and a
+    fresh FP32 filter, both run the next predict + update, and every output is
+    compared: parent log-likelihoods, per-measurement log normalisers, fitted
+    mixtures (rows correspond one to one) and merged mixtures (rows paired by
+    nearest mean).
+    (2) Trajectories at full size: FP64 and FP32 runs on the same seed and an FP64
+    run on a second seed; once resampling differs the runs are different Monte-Carlo
+    realisations, so the FP32-FP64 differences of OSPA and calibration error are
+    set against the FP64 seed-to-seed spread."""
+    import torch
+    dev = torch.device("cuda", 0)
+    DT = pkg.scene.DT
+    n_frames = args.precision_frames
+    # ---- (1) one-step errors
+    sc, cfg64 = pkg.scene.workload("precision_c3", precision=pkg.SCPHD_FP64, n_frames=n_frames)
+    cfg64.n_parents = 256
+    cfg32 = cfg64.copy()
+    cfg32.precision = pkg.SCPHD_FP32
+    src = pkg.SCPHDCameraCalibration(cfg64)
+    A = pkg.SCPHDCameraCalibration(cfg64)
+    B = pkg.SCPHDCameraCalibration(cfg32)
+    checkpoints = [k for k in (1, 3, 10, 30, 100, 200, n_frames - 2) if k < n_frames - 1]
+    local = []
+    for k in range(n_frames - 1):
+        z = sc.frames[k]
+        src.step(DT, z[:, 0], z[:, 1], sc.fixed[k], d=z[:, 2])
+        if k not in checkpoints:
+            continue
+        state = _capture_state(src)
+        zn = sc.frames[k + 1]
+        outs = []
+        for f in (A, B):
+            f.set_state(*state)
+            f.predict(DT)
+            f.update(zn[:, 0], zn[:, 1], sc.fixed[k + 1], d=zn[:, 2])
+            ell, ll = f.normalizers(len(zn))
+            outs.append((ell, ll, [f.mixture(pkg.SCPHD_MIX_FITTED, p) for p in range(f.n_parents)],
+                         [f.mixture(pkg.SCPHD_MIX_MERGED, p) for p in range(f.n_parents)], f.map_sizes()))
+        (e64, l64, F64, M64, n64), (e32, l32, F32, M32, n32) = outs
+        fm, fv, fw, mm, mv, same = [], [], [], [], [], 0
+        for a, b in zip(F64, F32):
+            live = (a[:, 1] > 0) & (a[:, 0] > 0)
+            if live.any() and a.shape == b.shape:
+                sd = np.sqrt(np.maximum(a[live][:, [8, 10, 13, 17, 22, 28]], 1e-30))
+                fm.append((np.abs(b[live][:, 2:8] - a[live][:, 2:8]) / sd).ravel())
+                fv.append((np.abs(b[live][:, [8, 10, 13, 17, 22, 28]] - a[live][:, [8, 10, 13, 17, 22, 28]])
+                           / np.maximum(np.abs(a[live][:, [8, 10, 13, 17, 22, 28]]), 1e-30)).ravel())
+                fw.append(np.abs(b[live, 0] - a[live, 0]) / a[live, 0])
+        for a, b in zip(M64, M32):
+            same += a.shape == b.shape
+            dm, dv = _match_rows(a, b, list(range(1, 7)), [7, 9, 12, 16, 21, 27])
+            mm.append(dm)
+            mv.append(dv)
+        cat = lambda xs: np.concatenate(xs) if xs and sum(len(x) for x in xs) else np.zeros(1)
+        q = lambda x: {"p50": float(np.percentile(x, 50)), "p99": float(np.percentile(x, 99)),
+                       "max": float(np.max(x))}
+        lrel = np.abs(l32 - l64) / np.maximum(1.0, np.abs(l64))
+        local.append({"frame": k + 1, "loglik_rel": q(lrel), "log_normaliser_abs": q(np.abs(e32 - e64)),
+                      "fitted_weight_rel": q(cat(fw)), "fitted_mean_sd": q(cat(fm)), "fitted_var_rel": q(cat(fv)),
+                      "merged_mean_sd": q(cat(mm)), "merged_var_rel": q(cat(mv)),
+                      "merged_count_equal_frac": same / len(M64),
+                      "map_size_equal_frac": float(np.mean(n32 == n64))})
+    for f in (src, A, B):
+        f.close()
+    # ---- (2) trajectories at full size
+    traj = {}
+    for name, prec, seed_off in (("fp64", pkg.SCPHD_FP64, 0), ("fp32", pkg.SCPHD_FP32, 0),
+                                 ("fp64_seed2", pkg.SCPHD_FP64, 1)):
+        sc, cfg = pkg.scene.workload("precision_c3", precision=prec, n_frames=n_frames)
+        cfg.seed = int(cfg.seed) + 7919 * seed_off
+        if args.parents:
+            cfg.n_parents = args.parents
+        f = pkg.SCPHDCameraCalibration(cfg)
+        dz = [torch.tensor(np.ascontiguousarray(z.T), dtype=torch.float64, device=dev) for z in sc.frames]
+        torch.cuda.synchronize()
+        rows, idx, t_dev = [], [], 0.0
+        for k in range(n_frames):
+            z = dz[k]
+            t0 = time.perf_counter()
+            f.predict(DT)
+            f.update_device(z[0].data_ptr(), z[1].data_ptr(), z[2].data_ptr(), z.shape[1], sc.fixed[k])
+            f.synchronize()
+            t_dev += time.perf_counter() - t0
+            st, lw = f.particles()
+            m = pkg.evaluate.frame_metrics(st, lw, f.map_weights, lambda p: f.map_clouds(p)[0], sc, k)
+            pose = pkg.evaluate.expected_pose(st, lw)
+            rows.append([m["ospa"], m["calib_position_m"], m["calib_angle_rad"], m["n_features"],
+                         m["cardinality"], *pose[[0, 1, 2, 6, 7, 8]]])
+            t0 = time.perf_counter()
+            f.resample()
+            f.synchronize()
+            t_dev += time.perf_counter() - t0
+            if k < 16:
+                idx.append(f.resample_indices().copy())
+        traj[name] = {"rows": np.array(rows), "idx": idx, "seconds": t_dev}
+        f.close()
+        del dz
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    a, b, c = traj["fp64"], traj["fp32"], traj["fp64_seed2"]
+    aligned = 0
+    for k in range(min(len(a["idx"]), len(b["idx"]))):
+        if not np.array_equal(a["idx"][k], b["idx"][k]):
+            break
+        aligned = k + 1
+    tail = slice(n_frames // 2, None)
+    mean = lambda r, j: float(r["rows"][tail, j].mean())
+    summ = {"frames": n_frames, "one_step": local, "resampling_identical_frames": aligned}
+    for j, nm in ((0, "ospa"), (1, "calib_position_m"), (2, "calib_angle_rad"), (3, "n_features")):
+        summ[nm] = {"fp64": mean(a, j), "fp32": mean(b, j), "fp64_seed2": mean(c, j),
+                    "fp32_minus_fp64": mean(b, j) - mean(a, j), "seed_spread_fp64": mean(c, j) - mean(a, j)}
+        summ[nm + "_final"] = {"fp64": float(a["rows"][-1, j]), "fp32": float(b["rows"][-1, j]),
+                               "fp64_seed2": float(c["rows"][-1, j])}
+    summ["seconds"] = {k2: v["seconds"] for k2, v in traj.items()}
+    summ["note"] = "trajectory figures are means over the second half of the frames"
+    if args.precision_dump:
+        np.savez_compressed(args.precision_dump, **{k2: v["rows"] for k2, v in traj.items()})
+    return summ
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -604,11 +760,17 @@ def main():
     ap.add_argument("--parents", type=int, default=0, help="override the parent count (profiling only)")
     ap.add_argument("--filters", type=int, default=64, help="filters of the batched_c2 workload")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="serving window of serving_c4")
+    ap.add_argument("--precision-frames", type=int, default=300, help="frames of the precision_c3 study")
+    ap.add_argument("--precision-dump", default="", help="npz of the per-frame trajectories")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "precision_c3":
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps({"workload": "precision_c3", "study": run_precision(args, load_package())}), flush=True)
     elif args.workload == "serving_c4":
         import torch
         torch.cuda.set_device(0)
