@@ -36,14 +36,10 @@ __host__ __device__ inline void philox(uint32_t c0, uint32_t c1, uint32_t c2, ui
                                        uint32_t k0, uint32_t k1, uint32_t out[4]) {
 #pragma unroll
     for (int r = 0; r < 10; ++r) {
-#ifdef __CUDA_ARCH__
-        uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
-        uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
-#else
-        uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
-        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
-        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
-#endif
+        // one 32x32 -> 64-bit product per multiplier gives both halves
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
         uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
         c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
         k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
@@ -102,7 +98,8 @@ template <> struct Pair<float> {
         float ua = __fmaf_rn((float)wa, 0x1p-32f, 0x1p-33f);
         float ub = __fmaf_rn((float)wb, 0x1p-32f, 0x1p-33f);
         ua = fminf(ua, 0.99999994f);
-        float r = sqrtf(-2.0f * __logf(ua));
+        const float r2 = -2.0f * __logf(ua);   // > 0: ua < 1
+        float r = r2 * rsqrtf(r2);
         float th = 6.283185307179586f * (ub - 0.5f);
         float s, c;
         __sincosf(th, &s, &c);
@@ -165,6 +162,17 @@ struct Model {   // measurement model constants (FP64 copy; kernels cast to T)
     double var[3];   // std_u^2, std_v^2, std_d^2
 };
 
+// Weight of a Gaussian's non-detection term, W (1 - mean pD), rounded step by step
+// (no contraction) so that the cloud-fit and merge kernels decide identically
+// whether the term survives the min_weight prune.
+__device__ __forceinline__ float nd_weight(float W, float pbar) { return __fmul_rn(W, __fsub_rn(1.0f, pbar)); }
+__device__ __forceinline__ double nd_weight(double W, double pbar) { return __dmul_rn(W, __dsub_rn(1.0, pbar)); }
+
+// Reciprocal in the transforms: correctly rounded in FP64; in FP32 the hardware
+// approximation (max 2 ulp), inside the FP32 mode's tolerance against FP64.
+__device__ __forceinline__ double trcp(double x) { return 1.0 / x; }
+__device__ __forceinline__ float trcp(float x) { return __fdividef(1.0f, x); }
+
 // world point -> (u, v, d, vu, vv, vd), computeMeasurement (:165-196) with baseline B
 template <typename T>
 __device__ inline void measure(const T X[6], const Pose<T>& P, const Model& m, T y[6]) {
@@ -176,7 +184,7 @@ __device__ inline void measure(const T X[6], const Pose<T>& P, const Model& m, T
     T vy = P.R[3] * X[3] + P.R[4] * X[4] + P.R[5] * X[5];
     T vz = P.R[6] * X[3] + P.R[7] * X[4] + P.R[8] * X[5];
     const T fx = (T)m.fx, fy = (T)m.fy, B = (T)m.B;
-    T iz = T(1) / z, iz2 = iz * iz;
+    T iz = trcp(z), iz2 = iz * iz;
     y[0] = (T)m.u0 - fx * iz * x;
     y[1] = (T)m.v0 - fy * iz * yy;
     y[2] = -fx * B * iz;
@@ -190,7 +198,7 @@ template <typename T>
 __device__ inline void invert(const T y[6], const Pose<T>& P, const Model& m, T X[6]) {
     const T fx = (T)m.fx, fy = (T)m.fy, B = (T)m.B, u0 = (T)m.u0, v0 = (T)m.v0;
     T u = y[0], v = y[1], d = y[2], vu = y[3], vv = y[4], vd = y[5];
-    T id = T(1) / d, id2 = id * id, r = fx / fy;
+    T id = trcp(d), id2 = id * id, r = fx / fy;
     T c0 = (u - u0) * B * id;
     T c1 = r * (v - v0) * B * id;
     T c2 = -fx * B * id;
@@ -269,21 +277,16 @@ __device__ inline T mahal6(const T* ma, const T* Sa, const T* mb, const T* Sb) {
     return dist;
 }
 
-// Measurement-independent Kalman terms of one fitted Gaussian for H = [I_K 0],
-// R = diag(var): S^-1, log-constant c = log pD + log w - K/2 log 2pi - 1/2 log det S,
-// gain K = P H' S^-1 and the Joseph-form posterior covariance
-// (I - K H) P (I - K H)' + K R K' of computeDetectionsKernel (src/kernels.cu:506-595),
-// which does not depend on the measurement.  Spread over a warp: every lane holds the fitted Gaussian (w, pD, packed
-// cov P); S, S^-1 and the log-constant are computed redundantly, the 18 gain entries
-// and the 21 Joseph-form covariance entries one per lane through the warp's shared
-// scratch sm (72 T), and the PD test of the posterior by every lane from shared
-// memory.  Writes the 47 prep values of this Gaussian to dst.
+// Measurement-independent Kalman terms of one fitted Gaussian, computed by one thread:
+// S = H P H' + R, S^-1, the log-constant log pD + log w - k/2 log 2pi - 1/2 log|S|,
+// the gain K = P H' S^-1 and the Joseph-form posterior covariance
+// P - K(HP) - (HP)'K' + K(HPH')K' + K R K' (src/kernels.cu:506-595), then the
+// posterior's PD test (isPosDef, src/device_math.cu:800-812).  P is the fitted
+// packed covariance, Pn scratch for the posterior (21 values); dst receives [0]
+// log-constant, [1] PD flag, [2..7] S^-1 packed, [8..25] K (6 x 3 row-major),
+// [26..46] posterior covariance packed.
 template <typename T, int K>
-__device__ inline void warp_kalman_prep(T w, T pdbar, const T* P, const Model& m, T* sm, int lane, T* dst) {
-    T* sP = sm;          // 21
-    T* sSi = sm + 21;    // 6
-    T* sK = sm + 27;     // 18 (row-major 6 x 3)
-    T* sPn = sm + 45;    // 21
+__device__ inline void kalman_prep(T w, T pdbar, const T* P, const Model& m, T* Pn, T* dst) {
     T S[6], Si[6];
     S[0] = P[0] + (T)m.var[0];
     S[1] = P[1];
@@ -308,57 +311,44 @@ __device__ inline void warp_kalman_prep(T w, T pdbar, const T* P, const Model& m
         cst = tlog(pdbar) + tlog(w) - T(0.5) * T(K) * log2pi - T(0.5) * tlog(det);
     else
         cst = tneg_inf<T>();
-    // stage P and S^-1 in shared memory
-    {
-        T v = P[0];
-#pragma unroll
-        for (int i = 1; i < 21; ++i) if (lane == i) v = P[i];
-        if (lane < 21) sP[lane] = v;
-        T u = Si[0];
-#pragma unroll
-        for (int i = 1; i < 6; ++i) if (lane == i) u = Si[i];
-        if (lane < 6) sSi[lane] = u;
-    }
-    __syncwarp();
     // gain entry q = r*3 + cc: K[r][cc] = sum_a P[r][a] S^-1[a][cc]
-    if (lane < 18) {
-        const int r = lane / 3, cc = lane - 3 * (lane / 3);
+    T Kg[18];
+#pragma unroll
+    for (int q = 0; q < 18; ++q) {
+        const int r = q / 3, cc = q % 3;
         T acc = 0;
         if (cc < K) {
 #pragma unroll
-            for (int a = 0; a < K; ++a) acc += sP[tri(r, a)] * sSi[tri(a, cc)];
+            for (int a = 0; a < K; ++a) acc += P[tri(r, a)] * Si[tri(a, cc)];
         }
-        sK[lane] = acc;
-        dst[kPrepK + lane] = acc;
+        Kg[q] = acc;
+        dst[kPrepK + q] = acc;
     }
-    __syncwarp();
-    // Joseph entry e = (ea, eb): P - K(HP) - (HP)'K' + K(HPH')K' + K R K'
-    if (lane < 21) {
+    // Joseph entry e = (ea, eb)
+#pragma unroll
+    for (int e = 0; e < 21; ++e) {
         int ea = 0;
-        while ((ea + 1) * (ea + 2) / 2 <= lane) ++ea;
-        const int eb = lane - ea * (ea + 1) / 2;
-        T s = sP[lane];
+        while ((ea + 1) * (ea + 2) / 2 <= e) ++ea;
+        const int eb = e - ea * (ea + 1) / 2;
+        T sv = P[e];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-            const T Kak = sK[ea * 3 + k], Kbk = sK[eb * 3 + k];
-            s -= Kak * sP[tri(k, eb)];
-            s -= sP[tri(ea, k)] * Kbk;
-            s += Kak * (T)m.var[k] * Kbk;
+            const T Kak = Kg[ea * 3 + k], Kbk = Kg[eb * 3 + k];
+            sv -= Kak * P[tri(k, eb)];
+            sv -= P[tri(ea, k)] * Kbk;
+            sv += Kak * (T)m.var[k] * Kbk;
 #pragma unroll
-            for (int l = 0; l < K; ++l) s += Kak * sP[tri(k, l)] * sK[eb * 3 + l];
+            for (int l = 0; l < K; ++l) sv += Kak * P[tri(k, l)] * Kg[eb * 3 + l];
         }
-        sPn[lane] = s;
-        dst[kPrepCov + lane] = s;
+        Pn[e] = sv;
+        dst[kPrepCov + e] = sv;
     }
-    __syncwarp();
     T L[21];
-    const bool pdok = chol6(sPn, L);
-    if (lane == 0) {
-        dst[0] = cst;
-        dst[1] = pdok ? T(1) : T(0);
-    }
-    if (lane < 6) dst[kPrepSi + lane] = sSi[lane];
-    __syncwarp();
+    const bool pdok = chol6(Pn, L);
+    dst[0] = cst;
+    dst[1] = pdok ? T(1) : T(0);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) dst[kPrepSi + q] = Si[q];
 }
 
 // log-likelihood exponent term c - 1/2 nu' S^-1 nu for measurement z

@@ -171,6 +171,7 @@ public:
     void* arena_ptr = nullptr;
     T* dump = nullptr;        // Gcap x 7 x Ps cloud dump scratch
     size_t merge_smem = 0;
+    size_t fit_smem = 0;
 
     ~Filter() override {
         if (stream) cudaStreamSynchronize(stream);
@@ -233,13 +234,16 @@ public:
         carve(a);
         CUDA_TRY(cudaMemsetAsync(p, 0, probe.used, stream));
         merge_smem = merge_smem_bytes<T>(prm.Scap, prm.Gcap, 4);
+        fit_smem = cloud_fit_smem_bytes<T>(prm.Ps);
         if (merge_smem > 227 * 1024)
             return fail(SCPHD_ERR_CAPACITY, "max_survivors/max_gaussians need " + std::to_string(merge_smem) +
                                                 " bytes of shared memory per merge block (limit 227 KB)");
         if (prm.K == 2) {
             CUDA_TRY(allow_dynamic_smem((const void*)k_merge<T, 2>));
+            CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit<T, 2>));
         } else {
             CUDA_TRY(allow_dynamic_smem((const void*)k_merge<T, 3>));
+            CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit<T, 3>));
         }
         const int N = prm.N;
         k_prior<<<(N + 255) / 256, 256, 0, stream>>>(prm, b.ext, b.lw);
@@ -284,7 +288,7 @@ public:
         const int N = prm.N;
         CUDA_TRY(cudaMemsetAsync(b.counters + 4, 0, 2 * sizeof(unsigned long long), stream));
         int h = stage_begin(1);
-        k_cloud_fit<T, K><<<N, 256, 0, stream>>>(prm, b, cur, M, fixed, pending ? 1 : 0, pending_dt, pending_frame,
+        k_cloud_fit<T, K><<<N, 256, fit_smem, stream>>>(prm, b, cur, M, fixed, pending ? 1 : 0, pending_dt, pending_frame,
                                                   sample_frame[cur], M > 0 ? d_stage : nullptr,
                                                   M > 0 ? d_stage + M : nullptr, M > 0 ? d_stage + 2 * M : nullptr);
         LAUNCHED();
@@ -1039,6 +1043,7 @@ template <typename T> struct Batch final : scphd_batch {
     std::vector<size_t> stage_off;
     size_t stage_total = 0;
     size_t merge_smem = 0;
+    size_t fit_smem = 0;
     void* dev_mem = nullptr;
 
     ~Batch() override {
@@ -1089,6 +1094,7 @@ template <typename T> struct Batch final : scphd_batch {
                 stage_off[first + i] = stage_total;
                 stage_total += 3 * (size_t)pr.Mcap;
                 merge_smem = std::max(merge_smem, merge_smem_bytes<T>(pr.Scap, pr.Gcap, 4));
+                fit_smem = std::max(fit_smem, cloud_fit_smem_bytes<T>(pr.Ps));
             }
             g.n_parent = (int)mp.back().size();
             g.n_pred = (int)mpred.back().size();
@@ -1122,8 +1128,10 @@ template <typename T> struct Batch final : scphd_batch {
         if (merge_smem > 227 * 1024) return fail(SCPHD_ERR_CAPACITY, "batch merge needs more than 227 KB of shared memory");
         if (K == 2) {
             CUDA_TRY(allow_dynamic_smem((const void*)k_merge_batch<T, 2>));
+            CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit_batch<T, 2>));
         } else {
             CUDA_TRY(allow_dynamic_smem((const void*)k_merge_batch<T, 3>));
+            CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit_batch<T, 3>));
         }
         // members now issue on the batch stream
         for (scphd_filter* f : fs) {
@@ -1142,7 +1150,7 @@ template <typename T> struct Batch final : scphd_batch {
             LAUNCHED();
         }
         for (const Group& g : groups) {
-            k_cloud_fit_batch<T, KK><<<g.n_parent, 256, 0, stream>>>(*g.tab, d_fa + g.first, g.map_parent);
+            k_cloud_fit_batch<T, KK><<<g.n_parent, 256, fit_smem, stream>>>(*g.tab, d_fa + g.first, g.map_parent);
             LAUNCHED();
         }
         for (const Group& g : groups) {

@@ -142,22 +142,107 @@ __global__ void k_predict_parents(__grid_constant__ const Params prm, double* ex
 // (.cu:1602-1609), normalizeWeightsKernel + fitGaussiansKernel (kernels.cu:996-1018,
 // 102-438) and the non-detection copy (.cu:1290-1420).
 //
-// Samples stream through registers: each is generated (merged component: drawn from
-// its stored Gaussian with the counter-based stream; non-detection cloud: loaded),
-// predicted, transformed, and folded into one-pass moments about a shift (the
-// warp's first sample).  With w'_s = omega_s pD_s and S0 = sum w', the reference's
-// normalised weights are w'_s / S0, so mean = shift + S1/S0 and the weighted
-// covariance is (SS/S0 - d d') (1 + S2/S0^2) with d = S1/S0, S2 = sum w'^2 (the
-// (W^2 + SS)/W normaliser of kernels.cu:196 with W = 1).  When S0 = 0 the
-// reference weights every sample by 1; that fit matters only when the mean pD is
-// positive (some sample weight omega = 0), and is then recomputed in a second pass.
-// A non-detection cloud is kept only if W (1 - pD_mean) >= min_weight, which needs
-// W >= min_weight: clouds with W >= min_weight are written while streaming and the
-// new map references only the retained ones.
+// Each sample is generated (merged component: drawn from its stored Gaussian with
+// the counter-based stream; non-detection cloud: loaded), predicted, transformed,
+// and staged in the warp's shared-memory rows as d = y - shift (shift: the warp's
+// first sample, if finite) with its weight w'_s = omega_s pD_s.  The 29 moments are
+// then summed lane by lane (lane q owns moment q: S0 = sum w', S2 = sum w'^2,
+// S1 = sum w' d, SS = sum w' d d'), so no per-lane accumulators live through the
+// sample loop.  With the reference's normalised weights w'_s / S0, mean = shift +
+// S1/S0 and the weighted covariance is (SS/S0 - d d') (1 + S2/S0^2), d = S1/S0 (the
+// (W^2 + SS)/W normaliser of kernels.cu:196 with W = 1).  Zero-weight samples do not
+// enter the sums (their staged d is cleared).  When S0 = 0 the reference weights
+// every sample by 1; that fit matters only when the mean pD is positive (some sample
+// weight omega = 0), and is computed from the staged rows.  A non-detection cloud is
+// kept only if W (1 - pD_mean) >= min_weight (nd_weight, the merge's test), which needs
+// W >= min_weight: clouds with W >= min_weight are written while streaming (with
+// evict-first stores: they are read again only next frame) and the new map references
+// only the retained ones.  (About 90 % of written clouds pass the prune at plain_c1
+// scale; staging the points to write only those costs more than it saves.)
+
+// y = L z + mean, with L (packed lower, 21) and the mean (6) read from the warp's
+// shared line in 16-byte pieces, consumed in packed order (row a, column c)
+template <typename T, typename V, int W>
+__device__ __forceinline__ void ltz_line(const T* line, const T z[6], T y[6]) {
+    const V* v = reinterpret_cast<const V*>(line);
+#pragma unroll
+    for (int a = 0; a < 6; ++a) y[a] = 0;
+#pragma unroll
+    for (int i = 0; i < 28 / W; ++i) {
+        const V q = v[i];
+        const T* e = reinterpret_cast<const T*>(&q);
+#pragma unroll
+        for (int h = 0; h < W; ++h) {
+            const int k = i * W + h;
+            if (k < 21) {
+                int a = 0;
+                while ((a + 1) * (a + 2) / 2 <= k) ++a;
+                y[a] += e[h] * z[k - a * (a + 1) / 2];
+            } else if (k < 27) {
+                y[k - 21] += e[h];
+            }
+        }
+    }
+}
+__device__ __forceinline__ void ltz_plus_mean(const float* line, const float z[6], float y[6]) {
+    ltz_line<float, float4, 4>(line, z, y);
+}
+__device__ __forceinline__ void ltz_plus_mean(const double* line, const double z[6], double y[6]) {
+    ltz_line<double, double2, 2>(line, z, y);
+}
+
+// sum over s < n (n a multiple of 4) of w[s] a[s] b[s], four partial sums, rows read
+// in 16-byte pieces (row starts are 16-byte aligned)
+__device__ __forceinline__ float moment_sweep(const float* w, const float* a, const float* b, int n) {
+    const float4* w4 = reinterpret_cast<const float4*>(w);
+    const float4* a4 = reinterpret_cast<const float4*>(a);
+    const float4* b4 = reinterpret_cast<const float4*>(b);
+    float s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    for (int i = 0; i < (n >> 2); ++i) {
+        const float4 x = w4[i], y = a4[i], z = b4[i];
+        s0 += x.x * y.x * z.x;
+        s1 += x.y * y.y * z.y;
+        s2 += x.z * y.z * z.z;
+        s3 += x.w * y.w * z.w;
+    }
+    return (s0 + s1) + (s2 + s3);
+}
+__device__ __forceinline__ double moment_sweep(const double* w, const double* a, const double* b, int n) {
+    const double2* w2 = reinterpret_cast<const double2*>(w);
+    const double2* a2 = reinterpret_cast<const double2*>(a);
+    const double2* b2 = reinterpret_cast<const double2*>(b);
+    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    for (int i = 0; i < (n >> 2); ++i) {
+        const double2 x = w2[2 * i], y = a2[2 * i], z = b2[2 * i];
+        const double2 x1 = w2[2 * i + 1], y1 = a2[2 * i + 1], z1 = b2[2 * i + 1];
+        s0 += x.x * y.x * z.x;
+        s1 += x.y * y.y * z.y;
+        s2 += x1.x * y1.x * z1.x;
+        s3 += x1.y * y1.y * z1.y;
+    }
+    return (s0 + s1) + (s2 + s3);
+}
+
+// Row stride of the staged samples, in elements: at least Ps, a multiple of 16 bytes,
+// and 12 words modulo 32 banks, so that the eight rows a lane-per-moment sweep reads
+// at one sample index fall in distinct banks.
+template <typename T> __host__ __device__ inline int stage_stride(int Ps) {
+    if (sizeof(T) == 4) return Ps + (((12 - Ps) % 32) + 32) % 32;
+    return Ps + (((6 - Ps) % 16) + 16) % 16;
+}
+constexpr int kFitWarps = 8;
+constexpr int kStageRows = 8;   // d[6], w', ones
+template <typename T> __host__ __device__ inline size_t cloud_fit_smem_bytes(int Ps) {
+    const size_t stage = (size_t)kFitWarps * kStageRows * stage_stride<T>(Ps);   // sample rows
+    const size_t prep = (size_t)kFitWarps * 32 * 42;                             // per-thread Kalman scratch
+    return (stage > prep ? stage : prep) * sizeof(T);
+}
+
 template <typename T, int K>
 __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>& b, int cur, int M, int fixed,
                                                int has_pred, double dt, uint32_t pred_frame, uint32_t sample_frame,
-                                               const double* zu, const double* zv, const double* zd, int p) {
+                                               const double* zu, const double* zv, const double* zd, int p,
+                                               T* s_stage) {
     if (p == 0 && zu != nullptr) {   // this frame's measurements into the T layout (u, v, d)
         for (int mm = threadIdx.x; mm < M; mm += blockDim.x) {
             b.z[mm * 3 + 0] = (T)zu[mm];
@@ -168,10 +253,13 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int row = b.src[p];
     const int G = min(b.map_n[cur][row], prm.Gcap);
+    const int P = prm.P, Ps = prm.Ps;
+    const int sY = stage_stride<T>(Ps);
+    T* Y = s_stage + (size_t)warp * kStageRows * sY;   // rows 0-5 d, 6 w', 7 ones
     __shared__ Pose<T> pose_upd, pose_src;
     __shared__ int s_rd, s_wr;
-    __shared__ T s_km[8 * 72];   // per warp: P[21], S^-1[6], K[18], P'[21]
-    __shared__ T s_L[8 * 24];    // per warp: Cholesky factor of a merged component
+    __shared__ __align__(16) T s_L[kFitWarps * 28];   // per warp: Cholesky factor and mean of a merged component
+    __shared__ T s_fit[kFitWarps * 32];  // per warp: the fitted row (W, pD, mean[6], cov[21])
     if (threadIdx.x == 0) {
         double zero[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         pose_upd = make_pose<T>(fixed ? zero : b.ext + 12 * p);
@@ -182,189 +270,186 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
         s_rd = 0;
         s_wr = 0;
     }
+    for (int s = lane; s < sY; s += 32) Y[7 * sY + s] = T(1);
     __syncthreads();
     const Model& m = prm.model;
-    const int P = prm.P, Ps = prm.Ps;
     const T invP = T(1) / T(P);
     const T dtT = (T)dt, half_dt2 = T(0.5) * (T)dt * (T)dt;
-    T* Lw = s_L + warp * 24;
-    for (int j = warp; j < G; j += blockDim.x >> 5) {
+    T* Lw = s_L + warp * 28;
+    T* fitw = s_fit + warp * 32;
+    // moment owned by this lane: rows (ra, rb) of the weighted product w' * Y[ra] * Y[rb]
+    int ra = 7, rb = 7;
+    if (lane == 1) ra = 6;
+    else if (lane >= 2 && lane < 8) ra = lane - 2;
+    else if (lane >= 8 && lane < 29) {
+        int e = lane - 8, aa = 0;
+        while ((aa + 1) * (aa + 2) / 2 <= e) ++aa;
+        ra = aa;
+        rb = e - aa * (aa + 1) / 2;
+    }
+    const int P4 = (P + 3) & ~3;
+    for (int j = warp; j < G; j += kFitWarps) {
         const size_t erow = (size_t)row * prm.Gcap + j;
         const T* ent = b.map[cur] + erow * kRow;
         const int ref = b.map_ref[cur][erow];
         const T W = has_pred ? ent[0] * (T)prm.ps : ent[0];
         const T* cl_in = ref >= 0 ? b.cloud[cur] + (size_t)ref * 7 * Ps : nullptr;
-        if (ref < 0) {
-            T L[21];
-            chol6(ent + 7, L);
-            if (lane < 21) {
-                T v = L[0];
-#pragma unroll
-                for (int i = 1; i < 21; ++i) if (lane == i) v = L[i];
-                Lw[lane] = v;
-            }
-            __syncwarp();
+        if (ref < 0) {   // Cholesky factor (21, stored in the map row) and mean (6) of the merged component
+            if (lane < 21) Lw[lane] = ent[7 + lane];
+            else if (lane < 27) Lw[lane] = ent[1 + lane - 21];
+            else if (lane == 27) Lw[27] = T(0);
         } else if (lane == 0) {
             atomicAdd(&s_rd, 1);
         }
+        __syncwarp();
         const bool write_nd = W >= (T)prm.min_weight;
         T* cl_out = b.cloud[cur ^ 1] + ((size_t)p * prm.Gcap + j) * 7 * Ps;
         const uint32_t key_i = (uint32_t)(-1 - ref);
-        // sample s: world point after the pending prediction, and its sample weight
-        auto sample = [&](int s, T X[6], T& om) {
-            if (ref < 0) {   // merged component: draw (.cu:640-690) and map to world (.cu:1222-1286)
-                uint32_t w0[4], w1[4];
-                philox((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 0), prm.key0, prm.key1, w0);
-                philox((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 1), prm.key0, prm.key1, w1);
-                T z[6];
-                Pair<T>::two(w0[0], w0[1], z[0], z[1]);
-                Pair<T>::two(w0[2], w0[3], z[2], z[3]);
-                Pair<T>::two(w1[0], w1[1], z[4], z[5]);
-                T y[6];
-#pragma unroll
-                for (int a = 0; a < 6; ++a) {
-                    T v = 0;
-#pragma unroll
-                    for (int c = 0; c <= a; ++c) v += Lw[tri(a, c)] * z[c];
-                    y[a] = v + ent[1 + a];
-                }
-                invert(y, pose_src, m, X);
-                om = invP;
-            } else {         // non-detection cloud carried from the previous frame
-#pragma unroll
-                for (int a = 0; a < 6; ++a) X[a] = cl_in[a * Ps + s];
-                om = cl_in[6 * Ps + s];
-            }
-            if (has_pred) {   // predict_features with feature noise
-                uint32_t w[4];
-                philox((uint32_t)s, (uint32_t)j, (uint32_t)p, ctr_word3(pred_frame, ST_FEAT, 0), prm.key0, prm.key1, w);
-                T z[4];
-                Pair<T>::two(w[0], w[1], z[0], z[1]);
-                Pair<T>::two(w[2], w[3], z[2], z[3]);
-#pragma unroll
-                for (int q = 0; q < 3; ++q) {
-                    T a = (T)prm.feat_std[q] * z[q];
-                    X[q] = X[q] + X[q + 3] * dtT + a * half_dt2;
-                    X[q + 3] = X[q + 3] + a * dtT;
-                }
-            }
-        };
-        T shift[6] = {0, 0, 0, 0, 0, 0};
-        T S0 = 0, S2 = 0, S1[6] = {0, 0, 0, 0, 0, 0}, SS[21];
-#pragma unroll
-        for (int i = 0; i < 21; ++i) SS[i] = 0;
+        T shift[6];
         int n_in = 0;
+        bool any_w = false;
         for (int t = 0; t * 32 < P; ++t) {
             const int s = lane + 32 * t;
             const bool valid = s < P;
             T X[6], om = 0, y[6];
             if (valid) {
-                sample(s, X, om);
+                if (ref < 0) {   // merged component: draw (.cu:640-690) and map to world (.cu:1222-1286)
+                    uint32_t w0[4], w1[4];
+                    philox((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 0), prm.key0,
+                           prm.key1, w0);
+                    philox((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 1), prm.key0,
+                           prm.key1, w1);
+                    T z[6];
+                    Pair<T>::two(w0[0], w0[1], z[0], z[1]);
+                    Pair<T>::two(w0[2], w0[3], z[2], z[3]);
+                    Pair<T>::two(w1[0], w1[1], z[4], z[5]);
+                    T yy[6];
+                    ltz_plus_mean(Lw, z, yy);   // y = L z + mean from the warp's shared line
+                    invert(yy, pose_src, m, X);
+                    om = invP;
+                } else {         // non-detection cloud carried from the previous frame
+#pragma unroll
+                    for (int a2 = 0; a2 < 6; ++a2) X[a2] = cl_in[a2 * Ps + s];
+                    om = cl_in[6 * Ps + s];
+                }
+                if (has_pred) {   // predict_features with feature noise
+                    uint32_t w[4];
+                    philox((uint32_t)s, (uint32_t)j, (uint32_t)p, ctr_word3(pred_frame, ST_FEAT, 0), prm.key0,
+                           prm.key1, w);
+                    T z[4];
+                    Pair<T>::two(w[0], w[1], z[0], z[1]);
+                    Pair<T>::two(w[2], w[3], z[2], z[3]);
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        T a2 = (T)prm.feat_std[q] * z[q];
+                        X[q] = X[q] + X[q + 3] * dtT + a2 * half_dt2;
+                        X[q + 3] = X[q + 3] + a2 * dtT;
+                    }
+                }
                 measure(X, pose_upd, m, y);
             } else {
 #pragma unroll
-                for (int a = 0; a < 6; ++a) { X[a] = 0; y[a] = 0; }
+                for (int a2 = 0; a2 < 6; ++a2) { X[a2] = 0; y[a2] = 0; }
             }
             const bool inr = valid && in_range(y, m);
             const T pds = inr ? (T)m.pd : T(0);
             n_in += __popc(__ballot_sync(0xffffffffu, inr));
             if (t == 0) {   // shift: the warp's first sample (finite), else 0
 #pragma unroll
-                for (int a = 0; a < 6; ++a) {
-                    T v = __shfl_sync(0xffffffffu, y[a], 0);
-                    shift[a] = isfinite(v) ? v : T(0);
+                for (int a2 = 0; a2 < 6; ++a2) {
+                    T v = __shfl_sync(0xffffffffu, y[a2], 0);
+                    shift[a2] = isfinite(v) ? v : T(0);
                 }
             }
             if (valid && write_nd) {   // non-detection cloud candidate: predicted world point, weight 1 - pD
 #pragma unroll
-                for (int a = 0; a < 6; ++a) cl_out[a * Ps + s] = X[a];
-                cl_out[6 * Ps + s] = T(1) - pds;
+                for (int a2 = 0; a2 < 6; ++a2) __stcs(cl_out + a2 * Ps + s, X[a2]);
+                __stcs(cl_out + 6 * Ps + s, T(1) - pds);
             }
             const T wp = om * pds;
-            if (wp != T(0)) {   // zero-weight samples do not enter the sums
-                T d[6];
+            any_w |= wp != T(0);
+            if (s < sY) {
 #pragma unroll
-                for (int a = 0; a < 6; ++a) d[a] = y[a] - shift[a];
-                S0 += wp;
-                S2 += wp * wp;
-#pragma unroll
-                for (int a = 0; a < 6; ++a) S1[a] += wp * d[a];
-#pragma unroll
-                for (int a = 0; a < 6; ++a)
-#pragma unroll
-                    for (int c = 0; c <= a; ++c) SS[tri(a, c)] += wp * d[a] * d[c];
+                for (int a2 = 0; a2 < 6; ++a2) Y[a2 * sY + s] = valid ? y[a2] - shift[a2] : T(0);
+                Y[6 * sY + s] = wp;
             }
         }
         if (write_nd && lane == 0) atomicAdd(&s_wr, 1);
-        S0 = warp_sum(S0);
-        S2 = warp_sum(S2);
-#pragma unroll
-        for (int a = 0; a < 6; ++a) S1[a] = warp_sum(S1[a]);
-#pragma unroll
-        for (int i = 0; i < 21; ++i) SS[i] = warp_sum(SS[i]);
+        __syncwarp();
+        any_w = __any_sync(0xffffffffu, any_w);
         const T pbar = (T)((double)n_in * m.pd / (double)P);
-        T mu[6], cv[21];
-        if (S0 > T(0)) {
+        if (any_w) {
+            // zero-weight samples leave the sums (their d may be non-finite)
+            for (int s = lane; s < P; s += 32)
+                if (Y[6 * sY + s] == T(0)) {
+#pragma unroll
+                    for (int a2 = 0; a2 < 6; ++a2) Y[a2 * sY + s] = T(0);
+                }
+            __syncwarp();
+            // lane q < 29: moment q over the samples, four partial sums
+            const T mom = lane < 29 ? moment_sweep(Y + 6 * sY, Y + ra * sY, Y + rb * sY, P4) : T(0);
+            const T S0 = __shfl_sync(0xffffffffu, mom, 0), S2 = __shfl_sync(0xffffffffu, mom, 1);
             const T inv = T(1) / S0, scale = T(1) + S2 * inv * inv;
-            T d[6];
+            // lanes 2-7 hold S1 (the mean offsets), lanes 8-28 hold SS
+            const T dl = (lane >= 2 && lane < 8) ? mom * inv : T(0);
+            T da = 0, db = 0;
+            T dvals[6];
 #pragma unroll
-            for (int a = 0; a < 6; ++a) { d[a] = S1[a] * inv; mu[a] = shift[a] + d[a]; }
+            for (int a2 = 0; a2 < 6; ++a2) dvals[a2] = __shfl_sync(0xffffffffu, dl, 2 + a2);
 #pragma unroll
-            for (int a = 0; a < 6; ++a)
-#pragma unroll
-                for (int c = 0; c <= a; ++c) cv[tri(a, c)] = (SS[tri(a, c)] * inv - d[a] * d[c]) * scale;
-        } else if (pbar > T(0)) {
-            // every sample weighted 1 (exp(LOG0 - LOG0)): unnormalised mean and
-            // covariance x (P + P)/P over the valid samples
-            T U1[6] = {0, 0, 0, 0, 0, 0}, U2[21];
-#pragma unroll
-            for (int i = 0; i < 21; ++i) U2[i] = 0;
-            for (int t = 0; t * 32 < P; ++t) {
-                const int s = lane + 32 * t;
-                if (s < P) {
-                    T X[6], om, y[6];
-                    sample(s, X, om);
-                    measure(X, pose_upd, m, y);
-#pragma unroll
-                    for (int a = 0; a < 6; ++a) U1[a] += y[a];
-                }
+            for (int a2 = 0; a2 < 6; ++a2) {
+                if (ra == a2) da = dvals[a2];
+                if (rb == a2) db = dvals[a2];
             }
+            if (lane >= 2 && lane < 8) fitw[lane] = shift[lane - 2] + dl;
+            if (lane >= 8 && lane < 29) fitw[lane] = (mom * inv - da * db) * scale;
+        } else if (pbar > T(0)) {
+            // every sample weighted 1 (exp(LOG0 - LOG0)): unnormalised mean (sum of the
+            // samples) and covariance x (P + P)/P over the valid samples
+            T mu = 0;
+            if (lane < 6) {
+                for (int s = 0; s < P; ++s) mu += Y[lane * sY + s] + shift[lane];
+            }
+            T mus[6];
 #pragma unroll
-            for (int a = 0; a < 6; ++a) mu[a] = warp_sum(U1[a]);   // sum of y (weights 1)
-            for (int t = 0; t * 32 < P; ++t) {
-                const int s = lane + 32 * t;
-                if (s < P) {
-                    T X[6], om, y[6];
-                    sample(s, X, om);
-                    measure(X, pose_upd, m, y);
+            for (int a2 = 0; a2 < 6; ++a2) mus[a2] = __shfl_sync(0xffffffffu, mu, a2);
+            T cva = 0;
+            if (lane >= 8 && lane < 29) {
+                T ma = 0, mb = 0, sa = 0, sb = 0;
 #pragma unroll
-                    for (int a = 0; a < 6; ++a)
-#pragma unroll
-                        for (int c = 0; c <= a; ++c) U2[tri(a, c)] += (y[a] - mu[a]) * (y[c] - mu[c]);
+                for (int a2 = 0; a2 < 6; ++a2) {
+                    if (ra == a2) { ma = mus[a2]; sa = shift[a2]; }
+                    if (rb == a2) { mb = mus[a2]; sb = shift[a2]; }
                 }
+                for (int s = 0; s < P; ++s)
+                    cva += ((Y[ra * sY + s] + sa) - ma) * ((Y[rb * sY + s] + sb) - mb);
             }
             const T scale = (T(P) * T(P) + T(P)) / T(P);
-#pragma unroll
-            for (int i = 0; i < 21; ++i) cv[i] = warp_sum(U2[i]) * scale;
+            if (lane < 6) fitw[2 + lane] = mu;
+            if (lane >= 8 && lane < 29) fitw[lane] = cva * scale;
         } else {   // entirely out of view: never used downstream (its log-constant is -inf)
-#pragma unroll
-            for (int a = 0; a < 6; ++a) mu[a] = shift[a];
-#pragma unroll
-            for (int i = 0; i < 21; ++i) cv[i] = 0;
+            if (lane < 6) fitw[2 + lane] = shift[lane];
+            if (lane >= 8 && lane < 29) fitw[lane] = T(0);
         }
+        if (lane == 0) fitw[0] = W;
+        if (lane == 1) fitw[1] = pbar;
+        __syncwarp();
         // fitted row: lane q writes element q (W, pD, mean[6], packed cov[21])
         T* fr = b.fit + ((size_t)p * prm.Gcap + j) * kRow;
-        {
-            T v = W;
-            if (lane == 1) v = pbar;
+        if (lane < 29) fr[lane] = fitw[lane];
+        __syncwarp();
+    }
+    __syncthreads();
+    // measurement-independent Kalman terms, one thread per fitted Gaussian; the fitted
+    // covariance and the posterior are staged in the (now free) sample rows
+    {
+        T* sPk = s_stage + (size_t)threadIdx.x * 42;
+        for (int j = threadIdx.x; j < G; j += blockDim.x) {
+            const T* fr = b.fit + ((size_t)p * prm.Gcap + j) * kRow;
 #pragma unroll
-            for (int a = 0; a < 6; ++a) if (lane == 2 + a) v = mu[a];
-#pragma unroll
-            for (int i = 0; i < 21; ++i) if (lane == 8 + i) v = cv[i];
-            if (lane < 29) fr[lane] = v;
+            for (int q = 0; q < 21; ++q) sPk[q] = fr[8 + q];
+            kalman_prep<T, K>(fr[0], fr[1], sPk, m, sPk + 21, b.prep + ((size_t)p * prm.Gcap + j) * kPrep);
         }
-        warp_kalman_prep<T, K>(W, pbar, cv, m, s_km + warp * 72, lane,
-                               b.prep + ((size_t)p * prm.Gcap + j) * kPrep);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -376,20 +461,23 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
 
 
 template <typename T, int K>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
     k_cloud_fit(__grid_constant__ const Params prm, __grid_constant__ const Bufs<T> b, int cur, int M, int fixed,
                 int has_pred, double dt, uint32_t pred_frame, uint32_t sample_frame, const double* zu,
                 const double* zv, const double* zd) {
-    cloud_fit_body<T, K>(prm, b, cur, M, fixed, has_pred, dt, pred_frame, sample_frame, zu, zv, zd, blockIdx.x);
+    extern __shared__ __align__(16) unsigned char dsm_fit[];
+    cloud_fit_body<T, K>(prm, b, cur, M, fixed, has_pred, dt, pred_frame, sample_frame, zu, zv, zd, blockIdx.x,
+                         reinterpret_cast<T*>(dsm_fit));
 }
 
 template <typename T, int K>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
     k_cloud_fit_batch(const __grid_constant__ SlotTable<T> tab, const FrameArgs* fas, const int2* map) {
+    extern __shared__ __align__(16) unsigned char dsm_fit[];
     const int2 fp = map[blockIdx.x];
     const FrameArgs fa = fas[fp.x];
     cloud_fit_body<T, K>(tab.prm[fp.x], tab.b[fp.x], fa.cur, fa.M, fa.fixed, fa.has_pred, fa.dt, fa.pred_frame,
-                         fa.sample_frame, fa.zu, fa.zv, fa.zd, fp.y);
+                         fa.sample_frame, fa.zu, fa.zv, fa.zd, fp.y, reinterpret_cast<T*>(dsm_fit));
 }
 
 // ---------------------------------------------------------------- (c) likelihood
@@ -1182,7 +1270,7 @@ __device__ __forceinline__ void merge_body(const Params& prm, const Bufs<T>& b, 
             w = out[(size_t)e * kRow];
         } else {
             const T* fr = b.fit + ((size_t)p * prm.Gcap + (e - n_out)) * kRow;
-            T wnd = fr[0] * (T(1) - fr[1]);
+            const T wnd = nd_weight(fr[0], fr[1]);
             w = (wnd >= minw) ? wnd : T(-1);   // -1: not retained
         }
         s_w[e] = w;
@@ -1231,9 +1319,14 @@ __device__ __forceinline__ void merge_body(const Params& prm, const Bufs<T>& b, 
         const int pos = s_pos[e];
         const int nxt = (e + 1 < n_all) ? s_pos[e + 1] : total;
         if (nxt == pos) continue;   // not kept
-        if (e < n_out) {
+        if (e < n_out) {   // merged component: weight, mean and the Cholesky factor of its covariance
             const T* sr = out + (size_t)e * kRow;
-            for (int q = 0; q < 28; ++q) mo[(size_t)pos * kRow + q] = sr[q];
+            T L[21];
+            chol6(sr + 7, L);
+            T* dr = mo + (size_t)pos * kRow;
+            for (int q = 0; q < 7; ++q) dr[q] = sr[q];
+#pragma unroll
+            for (int q = 0; q < 21; ++q) dr[7 + q] = L[q];
             mr[pos] = -1 - e;
         } else {
             const int j = e - n_out;
@@ -1481,8 +1574,7 @@ __global__ void __launch_bounds__(256) k_materialize(Params prm, Bufs<T> b, int 
         const T* ent = b.map[cur] + erow * kRow;
         const int ref = b.map_ref[cur][erow];
         T W = ent[0];
-        T L[21];
-        if (ref < 0) chol6(ent + 7, L);
+        const T* L = ent + 7;   // merged component: Cholesky factor stored in the map row
         T* cl = dst + ((size_t)(only_p >= 0 ? 0 : p) * prm.Gcap + j) * 7 * Ps;
         for (int s = lane; s < P; s += 32) {
             T X[6], om;
