@@ -277,6 +277,54 @@ __device__ inline T mahal6(const T* ma, const T* Sa, const T* mb, const T* Sb) {
     return dist;
 }
 
+// FP32 form of the same distance: each pivot's reciprocal square root is taken once
+// and the factor, its inverse and the distance use multiplications (hardware rsqrt,
+// max 2 ulp), in the same summation order.  The FP64 form keeps the divisions.
+template <>
+__device__ inline float mahal6<float>(const float* ma, const float* Sa, const float* mb, const float* Sb) {
+    float S[21], L[21], Li[21], dlt[6], inv[6];
+#pragma unroll
+    for (int i = 0; i < 21; ++i) S[i] = Sa[i] + Sb[i];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) dlt[i] = ma[i] - mb[i];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+#pragma unroll
+        for (int j = 0; j <= i; ++j) {
+            float tmp = S[tri(i, j)];
+            if (i == j) {
+#pragma unroll
+                for (int k = 0; k < j; ++k) tmp -= L[tri(j, k)] * L[tri(j, k)];
+                inv[i] = rsqrtf(tmp);
+                L[tri(i, i)] = tmp * inv[i];
+            } else {
+#pragma unroll
+                for (int k = 0; k < j; ++k) tmp -= L[tri(i, k)] * L[tri(j, k)];
+                L[tri(i, j)] = tmp * inv[j];
+            }
+        }
+    }
+#pragma unroll
+    for (int col = 0; col < 6; ++col) {
+#pragma unroll
+        for (int i = col; i < 6; ++i) {
+            float val = (i == col) ? 1.0f : 0.0f;
+#pragma unroll
+            for (int j = col; j < i; ++j) val -= L[tri(i, j)] * Li[tri(j, col)];
+            Li[tri(i, col)] = val * inv[i];
+        }
+    }
+    float dist = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        float s = 0;
+#pragma unroll
+        for (int j = 0; j <= i; ++j) s += dlt[j] * Li[tri(i, j)];
+        dist += s * s;
+    }
+    return dist;
+}
+
 // Measurement-independent Kalman terms of one fitted Gaussian, computed by one thread:
 // S = H P H' + R, S^-1, the log-constant log pD + log w - k/2 log 2pi - 1/2 log|S|,
 // the gain K = P H' S^-1 and the Joseph-form posterior covariance

@@ -775,10 +775,10 @@ __host__ __device__ inline int merge_sort_cap(int S, int G) {
 
 template <typename T> inline size_t merge_smem_bytes(int S, int G, int nwarps) {
     const size_t cap = merge_sort_cap(S, G), nchunk = (S + 31) / 32;
-    return cap * (sizeof(T) + 8) + 6 * (size_t)S * sizeof(float) + 3 * (size_t)S * 4 + cap * 4 +
-           (size_t)(S + 1) * 4 + (size_t)(S + G) * 4 + (size_t)nwarps * nchunk * 4 + 2 * (size_t)S + 64;
+    const size_t pf = 6 * (size_t)S * sizeof(float), pos = (size_t)(S + G) * 4;   // pos aliases pf
+    return cap * (sizeof(T) + 8) + (pf > pos ? pf : pos) + 3 * (size_t)S * 4 + cap * 4 + (size_t)(S + 1) * 4 +
+           (size_t)nwarps * nchunk * 4 + 2 * (size_t)S + 64;
 }
-
 template <typename T>
 __device__ inline void carve_merge_smem(unsigned char* smem, int S, int G, T*& s_w, uint32_t*& s_key, int*& s_r,
                                         int*& s_pos, MergeScratch<T>& ms) {
@@ -787,14 +787,14 @@ __device__ inline void carve_merge_smem(unsigned char* smem, int S, int G, T*& s
     s_key = reinterpret_cast<uint32_t*>(s_w + cap);
     s_r = reinterpret_cast<int*>(s_key + cap);
     ms.pf = reinterpret_cast<float*>(s_r + cap);
-    ms.lab = reinterpret_cast<int*>(ms.pf + 6 * S);
+    s_pos = reinterpret_cast<int*>(ms.pf);   // positions are used only once the prefilter rows are dead
+    ms.lab = reinterpret_cast<int*>(ms.pf + (6 * S > S + G ? 6 * S : S + G));
     ms.cidx = ms.lab + S;
     ms.fill = ms.cidx + S;
     ms.perm = ms.fill + S;
     ms.start = ms.perm + cap;
-    s_pos = ms.start + S + 1;
     ms.nchunk = (S + 31) / 32;
-    ms.masks = reinterpret_cast<uint32_t*>(s_pos + S + G);
+    ms.masks = reinterpret_cast<uint32_t*>(ms.start + S + 1);
     ms.flag = reinterpret_cast<uint8_t*>(ms.masks + (blockDim.x / 32) * ms.nchunk);
     ms.is_center = ms.flag + S;
 }
@@ -1350,13 +1350,13 @@ __device__ __forceinline__ void merge_body(const Params& prm, const Bufs<T>& b, 
 }
 
 template <typename T, int K>
-__global__ void __launch_bounds__(128) k_merge(__grid_constant__ const Params prm, __grid_constant__ const Bufs<T> b,
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 3) k_merge(__grid_constant__ const Params prm, __grid_constant__ const Bufs<T> b,
                                                int cur, int M, int fixed) {
     merge_body<T, K>(prm, b, cur, M, fixed, blockIdx.x);
 }
 
 template <typename T, int K>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 3)
     k_merge_batch(const __grid_constant__ SlotTable<T> tab, const FrameArgs* fas, const int2* map) {
     const int2 fp = map[blockIdx.x];
     const FrameArgs fa = fas[fp.x];

@@ -123,7 +123,7 @@ WORKLOADS = {
     "plain_c0": dict(n_parents=256, n_landmarks=50, clutter=10.0, max_gaussians=64, frames=100, max_meas=128,
                      max_survivors=384),
     "plain_c1": dict(n_parents=4096, n_landmarks=200, clutter=50.0, max_gaussians=256, frames=500, max_meas=384,
-                     max_survivors=768),
+                     max_survivors=512),
     "precision_c3": dict(n_parents=16384, n_landmarks=400, clutter=100.0, max_gaussians=512, frames=300,
                          max_meas=768, max_survivors=1536),
 }
