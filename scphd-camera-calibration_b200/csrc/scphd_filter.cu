@@ -241,9 +241,11 @@ public:
         if (prm.K == 2) {
             CUDA_TRY(allow_dynamic_smem((const void*)k_merge<T, 2>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit<T, 2>));
+            CUDA_TRY(allow_dynamic_smem((const void*)k_likelihood<T, 2>));
         } else {
             CUDA_TRY(allow_dynamic_smem((const void*)k_merge<T, 3>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit<T, 3>));
+            CUDA_TRY(allow_dynamic_smem((const void*)k_likelihood<T, 3>));
         }
         const int N = prm.N;
         k_prior<<<(N + 255) / 256, 256, 0, stream>>>(prm, b.ext, b.lw);
@@ -295,9 +297,10 @@ public:
         stage_end(h);
         pending = false;
         if (M > 0) {
-            dim3 grid(N, (M + 127) / 128);
+            const int bs = likelihood_block(M);
+            dim3 grid(N, (M + bs - 1) / bs);
             h = stage_begin(2);
-            k_likelihood<T, K><<<grid, 128, 0, stream>>>(prm, b, cur, M);
+            k_likelihood<T, K><<<grid, bs, likelihood_smem_bytes<T>(prm.Gcap), stream>>>(prm, b, cur, M);
             LAUNCHED();
             stage_end(h);
         }
@@ -1044,6 +1047,8 @@ template <typename T> struct Batch final : scphd_batch {
     size_t stage_total = 0;
     size_t merge_smem = 0;
     size_t fit_smem = 0;
+    size_t lik_smem = 0;
+    int lik_block = 32;
     void* dev_mem = nullptr;
 
     ~Batch() override {
@@ -1073,6 +1078,7 @@ template <typename T> struct Batch final : scphd_batch {
         std::vector<std::vector<int2>> mp, mpred;
         std::vector<std::vector<int4>> ml;
         stage_off.resize(F);
+        for (int f = 0; f < F; ++f) lik_block = std::max(lik_block, likelihood_block(fs[f]->prm.Mcap));
         for (int first = 0; first < F; first += kBatchSlots) {
             Group g;
             g.first = first;
@@ -1088,13 +1094,14 @@ template <typename T> struct Batch final : scphd_batch {
                 g.tab->b[i] = fl->b;
                 for (int q = 0; q < pr.N; ++q) mp.back().push_back(make_int2(i, q));
                 for (int q = 0; q < pr.N; q += 256) mpred.back().push_back(make_int2(i, q));
-                const int mb = (pr.Mcap + 127) / 128;
+                const int mb = (pr.Mcap + lik_block - 1) / lik_block;
                 for (int q = 0; q < pr.N; ++q)
                     for (int k = 0; k < mb; ++k) ml.back().push_back(make_int4(i, q, k, 0));
                 stage_off[first + i] = stage_total;
                 stage_total += 3 * (size_t)pr.Mcap;
                 merge_smem = std::max(merge_smem, merge_smem_bytes<T>(pr.Scap, pr.Gcap, 4));
                 fit_smem = std::max(fit_smem, cloud_fit_smem_bytes<T>(pr.Ps));
+                lik_smem = std::max(lik_smem, likelihood_smem_bytes<T>(pr.Gcap));
             }
             g.n_parent = (int)mp.back().size();
             g.n_pred = (int)mpred.back().size();
@@ -1129,9 +1136,11 @@ template <typename T> struct Batch final : scphd_batch {
         if (K == 2) {
             CUDA_TRY(allow_dynamic_smem((const void*)k_merge_batch<T, 2>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit_batch<T, 2>));
+            CUDA_TRY(allow_dynamic_smem((const void*)k_likelihood_batch<T, 2>));
         } else {
             CUDA_TRY(allow_dynamic_smem((const void*)k_merge_batch<T, 3>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit_batch<T, 3>));
+            CUDA_TRY(allow_dynamic_smem((const void*)k_likelihood_batch<T, 3>));
         }
         // members now issue on the batch stream
         for (scphd_filter* f : fs) {
@@ -1154,7 +1163,7 @@ template <typename T> struct Batch final : scphd_batch {
             LAUNCHED();
         }
         for (const Group& g : groups) {
-            k_likelihood_batch<T, KK><<<g.n_lik, 128, 0, stream>>>(*g.tab, d_fa + g.first, g.map_lik);
+            k_likelihood_batch<T, KK><<<g.n_lik, lik_block, lik_smem, stream>>>(*g.tab, d_fa + g.first, g.map_lik);
             LAUNCHED();
         }
         for (const Group& g : groups) {

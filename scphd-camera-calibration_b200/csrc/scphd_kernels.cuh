@@ -484,44 +484,71 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
 // Normaliser ell_{p,m} = logsumexp_j(log w_{j,m}) (+) log(M w0 + kappa)
 // (.cu:1729-1768) and survivor compaction: w_{j,m} = exp(log w - ell) >= min_weight
 // with a PD posterior (updateKernel, kernels.cu:622-657), births likewise.
+// One thread per measurement; a block covers the frame's measurements (a multiple
+// of 32 threads, up to 1024; more measurements take more blocks) and stages the
+// parent's Gaussian terms once in shared memory for both passes.
+constexpr int kLikTerms = 12;   // log-constant, PD flag, S^-1 (6), mean (3), pad: 16-byte pieces
+template <typename T> __host__ __device__ inline size_t likelihood_smem_bytes(int Gcap) {
+    return (size_t)Gcap * kLikTerms * sizeof(T);
+}
+__host__ __device__ inline int likelihood_block(int M) {
+    const int r = (M + 31) / 32 * 32;
+    return r < 32 ? 32 : (r > 1024 ? 1024 : r);
+}
+
+__device__ __forceinline__ void load_terms(const float* src, float* t) {
+    const float4* v = reinterpret_cast<const float4*>(src);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float4 q = v[i];
+        t[4 * i] = q.x; t[4 * i + 1] = q.y; t[4 * i + 2] = q.z; t[4 * i + 3] = q.w;
+    }
+}
+__device__ __forceinline__ void load_terms(const double* src, double* t) {
+    const double2* v = reinterpret_cast<const double2*>(src);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        const double2 q = v[i];
+        t[2 * i] = q.x; t[2 * i + 1] = q.y;
+    }
+}
+
 template <typename T, int K>
 __device__ __forceinline__ void likelihood_body(const Params& prm, const Bufs<T>& b, int cur, int M, int p,
-                                                int mblock) {
+                                                int mblock, T* s_terms) {
     const int m = mblock * blockDim.x + threadIdx.x;
     const int G = min(b.map_n[cur][b.src[p]], prm.Gcap);
-    __shared__ T s_c[128], s_pd[128], s_si[128][6], s_mu[128][3];
+    for (int jj = threadIdx.x; jj < G; jj += blockDim.x) {   // per Gaussian: c, pD flag, S^-1, mean, pad
+        const T* pr = b.prep + ((size_t)p * prm.Gcap + jj) * kPrep;
+        const T* fr = b.fit + ((size_t)p * prm.Gcap + jj) * kRow;
+        T* t = s_terms + (size_t)jj * kLikTerms;
+        t[0] = pr[0];
+        t[1] = pr[1];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) t[2 + i] = pr[kPrepSi + i];
+#pragma unroll
+        for (int a2 = 0; a2 < 3; ++a2) t[8 + a2] = fr[2 + a2];
+        t[11] = T(0);
+    }
     T zm[3] = {0, 0, 0};
     if (m < M) {
 #pragma unroll
-        for (int a = 0; a < K; ++a) zm[a] = b.z[m * 3 + a];
+        for (int a2 = 0; a2 < K; ++a2) zm[a2] = b.z[m * 3 + a2];
     }
     const T bpc = (T)log((double)M * prm.w0 + prm.kappa);
+    __syncthreads();
     T mx = tneg_inf<T>(), acc = 0;
-    for (int j0 = 0; j0 < G; j0 += 128) {
-        const int jj = j0 + threadIdx.x;
-        if (jj < G) {
-            const T* pr = b.prep + ((size_t)p * prm.Gcap + jj) * kPrep;
-            const T* fr = b.fit + ((size_t)p * prm.Gcap + jj) * kRow;
-            s_c[threadIdx.x] = pr[0];
-            s_pd[threadIdx.x] = pr[1];
-#pragma unroll
-            for (int i = 0; i < 6; ++i) s_si[threadIdx.x][i] = pr[kPrepSi + i];
-#pragma unroll
-            for (int a = 0; a < 3; ++a) s_mu[threadIdx.x][a] = fr[2 + a];
+    if (m < M) {
+        for (int k = 0; k < G; ++k) {
+            T t[kLikTerms];
+            load_terms(s_terms + (size_t)k * kLikTerms, t);
+            const T c = t[0];
+            // non-PD posteriors carry weight LOG0 before the normaliser (kernels.cu:597-598)
+            if (!(c > tneg_inf<T>()) || t[1] == T(0)) continue;
+            const T lt = log_term<T, K>(c, t + 2, t + 8, zm);
+            if (lt > mx) { acc = acc * texp(mx - lt) + T(1); mx = lt; }   // online log-sum-exp
+            else acc += texp(lt - mx);
         }
-        __syncthreads();
-        const int cnt = min(128, G - j0);
-        if (m < M) {
-            for (int k = 0; k < cnt; ++k) {
-                T c = s_c[k];
-                // non-PD posteriors carry weight LOG0 before the normaliser (kernels.cu:597-598)
-                if (!(c > tneg_inf<T>()) || s_pd[k] == T(0)) continue;
-                T lt = log_term<T, K>(c, s_si[k], s_mu[k], zm);
-                if (lt > mx) { acc = acc * texp(mx - lt) + T(1); mx = lt; }
-                else acc += texp(lt - mx);
-            }
-        }
-        __syncthreads();
     }
     T ell = bpc;
     if (m < M && mx > tneg_inf<T>()) {
@@ -533,47 +560,33 @@ __device__ __forceinline__ void likelihood_body(const Params& prm, const Bufs<T>
     // survivors
     const T minw = (T)prm.min_weight;
     const unsigned lane = threadIdx.x & 31;
-    for (int j0 = 0; j0 < G; j0 += 128) {
-        const int jj = j0 + threadIdx.x;
-        if (jj < G) {
-            const T* pr = b.prep + ((size_t)p * prm.Gcap + jj) * kPrep;
-            const T* fr = b.fit + ((size_t)p * prm.Gcap + jj) * kRow;
-            s_c[threadIdx.x] = pr[0];
-            s_pd[threadIdx.x] = pr[1];
-#pragma unroll
-            for (int i = 0; i < 6; ++i) s_si[threadIdx.x][i] = pr[kPrepSi + i];
-#pragma unroll
-            for (int a = 0; a < 3; ++a) s_mu[threadIdx.x][a] = fr[2 + a];
-        }
-        __syncthreads();
-        const int cnt = min(128, G - j0);
-        for (int k = 0; k < cnt; ++k) {
-            bool keep = false;
-            T w = 0;
-            if (m < M) {
-                T c = s_c[k];
-                if (c > tneg_inf<T>() && s_pd[k] > T(0)) {
-                    w = texp(log_term<T, K>(c, s_si[k], s_mu[k], zm) - ell);
-                    keep = w >= minw;
-                }
+    for (int k = 0; k < G; ++k) {
+        bool keep = false;
+        T w = 0;
+        if (m < M) {
+            T t[kLikTerms];
+            load_terms(s_terms + (size_t)k * kLikTerms, t);
+            const T c = t[0];
+            if (c > tneg_inf<T>() && t[1] > T(0)) {
+                w = texp(log_term<T, K>(c, t + 2, t + 8, zm) - ell);
+                keep = w >= minw;
             }
-            unsigned mask = __ballot_sync(0xffffffffu, keep);
-            if (mask) {
-                int base = 0;
-                if (lane == 0) base = atomicAdd(&b.surv_n[p], __popc(mask));
-                base = __shfl_sync(0xffffffffu, base, 0);
-                if (keep) {
-                    int slot = base + __popc(mask & ((1u << lane) - 1u));
-                    if (slot < prm.Scap) {
-                        b.surv_r[(size_t)p * prm.Scap + slot] = m * G + (j0 + k);
-                        b.surv_w[(size_t)p * prm.Scap + slot] = w;
-                    } else {
-                        atomicAdd(&b.counters[1], 1ull);
-                    }
+        }
+        unsigned mask = __ballot_sync(0xffffffffu, keep);
+        if (mask) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(&b.surv_n[p], __popc(mask));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (keep) {
+                int slot = base + __popc(mask & ((1u << lane) - 1u));
+                if (slot < prm.Scap) {
+                    b.surv_r[(size_t)p * prm.Scap + slot] = m * G + k;
+                    b.surv_w[(size_t)p * prm.Scap + slot] = w;
+                } else {
+                    atomicAdd(&b.counters[1], 1ull);
                 }
             }
         }
-        __syncthreads();
     }
     // birth term of measurement m (always PD)
     bool keep = false;
@@ -600,19 +613,21 @@ __device__ __forceinline__ void likelihood_body(const Params& prm, const Bufs<T>
 }
 
 template <typename T, int K>
-__global__ void __launch_bounds__(128) k_likelihood(__grid_constant__ const Params prm,
-                                                    __grid_constant__ const Bufs<T> b, int cur, int M) {
-    likelihood_body<T, K>(prm, b, cur, M, blockIdx.x, blockIdx.y);
+__global__ void __launch_bounds__(1024) k_likelihood(__grid_constant__ const Params prm,
+                                                     __grid_constant__ const Bufs<T> b, int cur, int M) {
+    extern __shared__ __align__(16) unsigned char dsm_lik[];
+    likelihood_body<T, K>(prm, b, cur, M, blockIdx.x, blockIdx.y, reinterpret_cast<T*>(dsm_lik));
 }
 
 // map entry: (filter, parent, measurement block); blocks past a filter's M exit
 template <typename T, int K>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(1024)
     k_likelihood_batch(const __grid_constant__ SlotTable<T> tab, const FrameArgs* fas, const int4* map) {
+    extern __shared__ __align__(16) unsigned char dsm_lik[];
     const int4 e = map[blockIdx.x];
     const int M = fas[e.x].M;
     if (e.z * (int)blockDim.x >= M) return;
-    likelihood_body<T, K>(tab.prm[e.x], tab.b[e.x], fas[e.x].cur, M, e.y, e.z);
+    likelihood_body<T, K>(tab.prm[e.x], tab.b[e.x], fas[e.x].cur, M, e.y, e.z, reinterpret_cast<T*>(dsm_lik));
 }
 
 // ---------------------------------------------------------------- (d) merge
