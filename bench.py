@@ -322,6 +322,14 @@ def run_b200(args):
     per_launch = algo_bytes / max(1, n_launch)
     avg_ms = stage_ms / max(1, n_launch)
     achieved = per_launch / (avg_ms / 1e3) / 1e9 if avg_ms > 0 else 0.0
+    # compute side: algorithmic FP32 flops (about 250 per cloud sample: draw, two
+    # camera transforms, prediction, moments) against the nominal FP32 CUDA-core peak
+    # (148 SMs x 128 lanes x 2 flops x 1.965 GHz); the stage is issue-bound, not HBM-bound
+    fp32_peak_tflops = 148 * 128 * 2 * 1.965e9 / 1e12
+    flops = {"cloud_fit": fitted * P * 250.0}.get(name, 0.0) / max(1, n_launch)
+    compute = {"flops_per_launch": flops, "achieved_tflops": flops / (avg_ms / 1e3) / 1e12 if avg_ms > 0 else 0.0,
+               "peak_tflops": fp32_peak_tflops, "peak_source": "nominal FP32 CUDA-core rate"}
+    compute["frac"] = compute["achieved_tflops"] / fp32_peak_tflops
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
@@ -356,7 +364,8 @@ def run_b200(args):
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                     "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": avg_ms},
+                     "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": avg_ms,
+                     "compute": compute},
         "stage_ms_per_frame": {k2: v[0] / max(1, v[1]) for k2, v in stages.items()},
         "cpu_baseline": cpu,
         "clocks": clk,
