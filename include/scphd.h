@@ -172,6 +172,9 @@ scphd_status scphd_set_state(scphd_filter* f, const double* states, const double
  * one parent (before the max_survivors cut); [14..15] reserved. */
 scphd_status scphd_get_counters(scphd_filter* f, int64_t counters[16]);
 
+/* The configuration the filter was created with. */
+scphd_status scphd_get_config(scphd_filter* f, scphd_config* out);
+
 /* The CUDA stream (a cudaStream_t) all of the handle's work is issued on, so a
  * caller can order its own work or timing events after the filter's. */
 void* scphd_stream(scphd_filter* f);

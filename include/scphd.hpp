@@ -4,14 +4,16 @@
 // only its include line and constructor argument changed.
 //
 //   reference                                   here
-//   SCPHDCameraCalibration(const char* cfg)     SCPHDCameraCalibration(const scphd_config&)
+//   SCPHDCameraCalibration(const char* cfg)     same (a libconfig file, scphd_config_from_file), or
+//                                               SCPHDCameraCalibration(const scphd_config&)
 //   void predict(double dt)                     same
 //   void update(vector<double> u,               same, plus an overload with a disparity
 //               vector<double> v, bool fixed)   vector for (u,v,d) measurements
 //   void resample()                             same
 //   void checkStuff()                           same: prints "nan weight detected" and
 //                                               exits with status 2 (src/.cu:812-821)
-//   void writeMat(const char*)                  particles()/weights()/mixture() accessors
+//   void writeMat(const char*)                  same (MAT level 5, scphd_write_mat), and the
+//                                               particles()/weights()/mixture() accessors
 //
 // Errors of the C ABI raise scphd::Error (the reference had no error reporting on
 // this path besides exit(2)).
@@ -19,6 +21,7 @@
 #define SCPHD_HPP
 
 #include "scphd.h"
+#include "scphd_io.h"
 
 #include <cmath>
 #include <cstdio>
@@ -46,6 +49,14 @@ public:
     explicit SCPHDCameraCalibration(const scphd_config& cfg) : cfg_(cfg) {
         scphd::check_status(scphd_create(&cfg_, &f_));
     }
+    // from a configuration file in the reference's libconfig syntax (library defaults
+    // for every key the file does not set)
+    explicit SCPHDCameraCalibration(const char* config_file) {
+        scphd_config_defaults(&cfg_);
+        scphd_run_options opts = {1 << 30, 0, 0, 0};
+        scphd::check_status(scphd_config_from_file(config_file, &cfg_, &opts));
+        scphd::check_status(scphd_create(&cfg_, &f_));
+    }
     ~SCPHDCameraCalibration() {
         if (f_) scphd_destroy(f_);
     }
@@ -70,6 +81,10 @@ public:
         int32_t r = 0;
         scphd::check_status(scphd_resample(f_, &r));
         return r != 0;
+    }
+
+    void writeMat(const char* path, bool save_all_maps = false) {
+        scphd::check_status(scphd_write_mat(f_, path, save_all_maps ? 1 : 0));
     }
 
     void checkStuff() {

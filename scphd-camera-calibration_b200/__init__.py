@@ -6,5 +6,6 @@ which registers it as the module `scphd_b200`.
 """
 from .scphd import (SCPHD_FP32, SCPHD_FP64, SCPHD_MIX_FITTED, SCPHD_MIX_MERGED,  # noqa: F401
                     JOB_DONE, JOB_QUEUED, JOB_RUNNING, SCPHDBatch, SCPHDCameraCalibration, SCPHDServer, ScphdConfig, ScphdError, ScphdFrame, kernel_launches,
-                    device_bytes, load_library, merge_components, reference_defaults, systematic_resample)
+                    config_from_file, device_bytes, load_library, merge_components, read_mat_frames,
+                    write_mat_arrays, reference_defaults, systematic_resample)
 from . import evaluate, scene  # noqa: F401

@@ -10,8 +10,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(CSRC, "libscphd_b200.so")
-SOURCES = ["scphd_filter.cu", "scphd_server.cu"]
-DEPS = SOURCES + ["scphd_kernels.cuh", "scphd_device.cuh"]
+CLI = os.path.join(CSRC, "scphd_calibrate")   # command-line driver (links LIB)
+SOURCES = ["scphd_filter.cu", "scphd_server.cu", "scphd_io.cpp"]
+DEPS = SOURCES + ["scphd_kernels.cuh", "scphd_device.cuh", "scphd_cli.cpp"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -28,10 +29,11 @@ def nvcc() -> str:
 
 
 def stale() -> bool:
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(CLI):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, d) for d in DEPS] + [os.path.join(ROOT, "include", "scphd.h")]
+    deps = [os.path.join(CSRC, d) for d in DEPS] + [os.path.join(ROOT, "include", h)
+                                                    for h in ("scphd.h", "scphd_io.h")]
     return any(os.path.getmtime(d) > t for d in deps)
 
 
@@ -39,7 +41,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not stale():
         return LIB
     cmd = [nvcc(), *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-o", LIB,
-           *[os.path.join(CSRC, s) for s in SOURCES]]
+           *[os.path.join(CSRC, s) for s in SOURCES], "-lz"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     res = subprocess.run(cmd, capture_output=True, text=True)
@@ -48,7 +50,20 @@ def build(force: bool = False, verbose: bool = False) -> str:
         raise RuntimeError("nvcc failed building libscphd_b200.so")
     if verbose:
         sys.stderr.write(res.stderr)
+    build_cli()
     return LIB
+
+
+def build_cli() -> str:
+    """The command-line driver: host C++ over the C ABI, rpath to the library beside it."""
+    cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+    cmd = [cxx, "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), os.path.join(CSRC, "scphd_cli.cpp"),
+           "-L", CSRC, "-lscphd_b200", "-Wl,-rpath,$ORIGIN", "-o", CLI]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("g++ failed building scphd_calibrate")
+    return CLI
 
 
 if __name__ == "__main__":

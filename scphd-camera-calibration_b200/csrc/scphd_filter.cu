@@ -767,6 +767,12 @@ scphd_status scphd_set_state(scphd_filter* f, const double* states, const double
     return f->set_state(states, log_weights, sizes, weights, clouds, omega);
 }
 
+scphd_status scphd_get_config(scphd_filter* f, scphd_config* out) {
+    if (!f || !out) return fail(SCPHD_ERR_INVALID, "null argument");
+    *out = f->cfg;
+    return SCPHD_OK;
+}
+
 scphd_status scphd_get_counters(scphd_filter* f, int64_t counters[16]) {
     HANDLE(f);
     if (!counters) return fail(SCPHD_ERR_INVALID, "null output");

@@ -87,6 +87,12 @@ class ScphdConfig(ctypes.Structure):
         return out
 
 
+class ScphdRunOptions(ctypes.Structure):
+    """scphd_run_options: driver settings read from a configuration file."""
+    _fields_ = [("max_steps", ctypes.c_int32), ("slam", ctypes.c_int32), ("save_all_maps", ctypes.c_int32),
+                ("verbosity", ctypes.c_int32)]
+
+
 class ScphdFrame(ctypes.Structure):
     """scphd_frame: one filter's measurements for a batched step."""
     _fields_ = [("u", ctypes.c_void_p), ("v", ctypes.c_void_p), ("d", ctypes.c_void_p),
@@ -187,6 +193,12 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "scphd_server_job_result": (i32, [vp, i64, P(d), P(d)]),
         "scphd_server_stats": (i32, [vp, P(i64)]),
         "scphd_server_step_times": (i32, [vp, i64, i32, P(d), P(i32), P(i32)]),
+        "scphd_get_config": (i32, [vp, P(ScphdConfig)]),
+        "scphd_config_from_file": (i32, [ctypes.c_char_p, P(ScphdConfig), P(ScphdRunOptions)]),
+        "scphd_read_mat_frames": (i32, [ctypes.c_char_p, ctypes.c_char_p, P(i32), P(i32), P(i32), P(d), i64]),
+        "scphd_write_mat": (i32, [vp, ctypes.c_char_p, i32]),
+        "scphd_write_mat_arrays": (i32, [ctypes.c_char_p, i32, P(ctypes.c_char_p), P(i32), P(i32),
+                                         P(P(d))]),
         "scphd_last_error": (ctypes.c_char_p, []),
         "scphd_kernel_launches": (i64, []),
     }
@@ -226,6 +238,58 @@ def device_bytes(config: ScphdConfig) -> int:
     out = ctypes.c_int64(0)
     _check(lib.scphd_device_bytes(ctypes.byref(config), ctypes.byref(out)))
     return int(out.value)
+
+
+def config_from_file(path: str, base: Optional[ScphdConfig] = None):
+    """Read a configuration file in the reference's libconfig syntax; returns the
+    filter configuration (starting from `base` or the library defaults) and the
+    driver options {max_steps, slam, save_all_maps, verbosity}."""
+    lib = load_library()
+    cfg = base.copy() if base is not None else ScphdConfig()
+    if base is None:
+        lib.scphd_config_defaults(ctypes.byref(cfg))
+    opts = ScphdRunOptions(1 << 30, 0, 0, 0)
+    _check(lib.scphd_config_from_file(os.fsencode(path), ctypes.byref(cfg), ctypes.byref(opts)))
+    return cfg, {"max_steps": int(opts.max_steps), "slam": bool(opts.slam),
+                 "save_all_maps": bool(opts.save_all_maps), "verbosity": int(opts.verbosity)}
+
+
+def read_mat_frames(path: str, var: str):
+    """Frames of a MAT cell array of 2 x n or 3 x n matrices, as a list of (rows, n)
+    arrays (the reference's readMatfile)."""
+    lib = load_library()
+    n, rows = ctypes.c_int32(0), ctypes.c_int32(0)
+    _check(lib.scphd_read_mat_frames(os.fsencode(path), var.encode(), ctypes.byref(n), ctypes.byref(rows),
+                                     None, None, 0))
+    cap = 1 << 16
+    while True:
+        sizes = np.zeros(n.value, np.int32)
+        data = np.zeros(cap, np.float64)
+        st = lib.scphd_read_mat_frames(os.fsencode(path), var.encode(), ctypes.byref(n), ctypes.byref(rows),
+                                       _iptr(sizes), _dptr(data), cap)
+        if st == 3:   # capacity
+            cap *= 4
+            continue
+        _check(st)
+        break
+    out, at, r = [], 0, rows.value
+    for k in range(n.value):
+        out.append(data[at:at + r * sizes[k]].reshape(r, sizes[k]).copy())
+        at += r * sizes[k]
+    return out
+
+
+def write_mat_arrays(path: str, arrays: dict) -> None:
+    """Write named real matrices to a MAT file."""
+    lib = load_library()
+    items = [(k, np.asfortranarray(np.atleast_2d(np.asarray(v, np.float64)))) for k, v in arrays.items()]
+    n = len(items)
+    names = (ctypes.c_char_p * n)(*[k.encode() for k, _ in items])
+    rows = (ctypes.c_int32 * n)(*[a.shape[0] for _, a in items])
+    cols = (ctypes.c_int32 * n)(*[a.shape[1] for _, a in items])
+    ptrs = (ctypes.POINTER(ctypes.c_double) * n)(*[a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+                                                   for _, a in items])
+    _check(lib.scphd_write_mat_arrays(os.fsencode(path), n, names, rows, cols, ptrs))
 
 
 def kernel_launches() -> int:
@@ -303,6 +367,13 @@ class SCPHDCameraCalibration:
         _check(self._lib.scphd_step_device(self._h, float(dt), ctypes.c_void_p(u_ptr), ctypes.c_void_p(v_ptr),
                                            ctypes.c_void_p(d_ptr) if d_ptr else None, int(n),
                                            int(bool(fixed_camera))))
+
+    def writeMat(self, path: str, save_all_maps: bool = False) -> None:
+        """The reference's writeMat: particles, weights and the MAP parent's map (and
+        with save_all_maps the per-parent mixtures) to a MAT file."""
+        _check(self._lib.scphd_write_mat(self._h, os.fsencode(path), int(bool(save_all_maps))))
+
+    write_mat = writeMat
 
     def checkStuff(self) -> None:
         _check(self._lib.scphd_check(self._h))

@@ -11,7 +11,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def test_library_exports_every_declared_symbol(pkg):
-    hdr = open(os.path.join(ROOT, "include", "scphd.h")).read()
+    hdr = "".join(open(os.path.join(ROOT, "include", h)).read() for h in ("scphd.h", "scphd_io.h"))
     names = sorted(set(re.findall(r"\b(scphd_[a-z_0-9]+)\s*\(", hdr)))
     assert len(names) >= 20
     lib = pkg.load_library()
