@@ -684,26 +684,141 @@ template <typename T> __device__ __forceinline__ bool merge_before(T wa, uint32_
     return wa > wb || (wa == wb && ka < kb);
 }
 
-// In-place bitonic sort of (w, key, r) by merge_before over n_pad (power of 2) slots.
-template <typename T>
-__device__ void sort_survivors(T* s_w, uint32_t* s_key, int* s_r, int n_pad) {
-    for (int k = 2; k <= n_pad; k <<= 1) {
-        for (int jj = k >> 1; jj > 0; jj >>= 1) {
-            for (int i = threadIdx.x; i < n_pad; i += blockDim.x) {
-                int ixj = i ^ jj;
-                if (ixj > i) {
-                    bool up = (i & k) == 0;
-                    bool before = merge_before(s_w[ixj], s_key[ixj], s_w[i], s_key[i]);
-                    if (before == up) {
-                        T tw = s_w[i]; s_w[i] = s_w[ixj]; s_w[ixj] = tw;
-                        uint32_t tk = s_key[i]; s_key[i] = s_key[ixj]; s_key[ixj] = tk;
-                        int tr = s_r[i]; s_r[i] = s_r[ixj]; s_r[ixj] = tr;
-                    }
-                }
+// Bitonic sort of n_pad (a power of two) items in shared arrays, ordered by
+// Items::before.  The comparator network is the textbook one (for k = 2, 4, ..:
+// for j = k/2 .. 1: items i and i^j swap when the later should come first, in the
+// direction of bit k of i).  When the block splits the items into one chunk of 32 R
+// items per warp (R = 1..8), every stage whose partners lie in the same chunk runs in
+// registers (j < 32: shuffles across lanes; 32 <= j < 32 R: within a thread), and only
+// the stages with j >= 32 R go through shared memory, each behind a barrier; otherwise
+// every stage does.  Both give the network's result.  Starts and ends with a barrier.
+template <typename T> struct SurvItems {   // (weight, tie key, rank) by merge_before
+    T* w;
+    uint32_t* key;
+    int* r;
+    struct Item { T w; uint32_t key; int r; };
+    __device__ Item load(int i) const { return Item{w[i], key[i], r[i]}; }
+    __device__ void store(int i, const Item& x) const { w[i] = x.w; key[i] = x.key; r[i] = x.r; }
+    __device__ static bool before(const Item& a, const Item& b) { return merge_before(a.w, a.key, b.w, b.key); }
+    __device__ static Item shfl(const Item& x, int m) {
+        return Item{__shfl_xor_sync(0xffffffffu, x.w, m), __shfl_xor_sync(0xffffffffu, x.key, m),
+                    __shfl_xor_sync(0xffffffffu, x.r, m)};
+    }
+};
+struct KeyItems {   // (key, value) by ascending key
+    uint32_t* key;
+    int* val;
+    struct Item { uint32_t key; int val; };
+    __device__ Item load(int i) const { return Item{key[i], val[i]}; }
+    __device__ void store(int i, const Item& x) const { key[i] = x.key; val[i] = x.val; }
+    __device__ static bool before(const Item& a, const Item& b) { return a.key < b.key; }
+    __device__ static Item shfl(const Item& x, int m) {
+        return Item{__shfl_xor_sync(0xffffffffu, x.key, m), __shfl_xor_sync(0xffffffffu, x.val, m)};
+    }
+};
+
+// one shared-memory stage (k, j) over all pairs
+template <typename Items>
+__device__ __forceinline__ void bitonic_smem_stage(const Items& it, int n_pad, int k, int jj) {
+    for (int i = threadIdx.x; i < n_pad; i += blockDim.x) {
+        const int ixj = i ^ jj;
+        if (ixj > i) {
+            const bool up = (i & k) == 0;
+            const typename Items::Item lo = it.load(i), hi = it.load(ixj);
+            if (Items::before(hi, lo) == up) {
+                it.store(i, hi);
+                it.store(ixj, lo);
             }
-            __syncthreads();
         }
     }
+}
+
+// stage (k, j) with 32 <= j < 32 R: pairs (r, r | D) of one thread, D = j / 32
+template <int R, int D, typename Items>
+__device__ __forceinline__ void bitonic_thread_stage(typename Items::Item (&x)[R], int base, int lane, int k) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        if ((r & D) == 0 && (r | D) < R) {
+            const bool up = ((base + r * 32 + lane) & k) == 0;
+            if (Items::before(x[r | D], x[r]) == up) {
+                const typename Items::Item t = x[r];
+                x[r] = x[r | D];
+                x[r | D] = t;
+            }
+        }
+    }
+}
+
+// stages (k, j0), (k, j0/2), .., (k, 1), all inside the warp's chunk
+template <int R, typename Items>
+__device__ __forceinline__ void bitonic_local(typename Items::Item (&x)[R], int base, int lane, int k, int j0) {
+    for (int jj = j0; jj > 0; jj >>= 1) {
+        if (jj >= 32) {
+            const int d = jj >> 5;
+            if (d == 4) bitonic_thread_stage<R, 4, Items>(x, base, lane, k);
+            else if (d == 2) bitonic_thread_stage<R, 2, Items>(x, base, lane, k);
+            else bitonic_thread_stage<R, 1, Items>(x, base, lane, k);
+        } else {
+            const bool lower = (lane & jj) == 0;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const bool up = ((base + r * 32 + lane) & k) == 0;
+                const typename Items::Item q = Items::shfl(x[r], jj);
+                const bool sw = lower ? (Items::before(q, x[r]) == up) : (Items::before(x[r], q) == up);
+                if (sw) x[r] = q;
+            }
+        }
+    }
+}
+
+template <int R, typename Items>
+__device__ void bitonic_sort_chunks(const Items& it, int n_pad) {
+    const int lane = threadIdx.x & 31;
+    const int CH = 32 * R, base = (threadIdx.x >> 5) * CH;
+    typename Items::Item x[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) x[r] = it.load(base + r * 32 + lane);
+    for (int k = 2; k <= CH; k <<= 1) bitonic_local<R, Items>(x, base, lane, k, k >> 1);
+#pragma unroll
+    for (int r = 0; r < R; ++r) it.store(base + r * 32 + lane, x[r]);
+    for (int k = 2 * CH; k <= n_pad; k <<= 1) {
+        for (int jj = k >> 1; jj >= CH; jj >>= 1) {
+            __syncthreads();
+            bitonic_smem_stage(it, n_pad, k, jj);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < R; ++r) x[r] = it.load(base + r * 32 + lane);
+        bitonic_local<R, Items>(x, base, lane, k, CH >> 1);
+#pragma unroll
+        for (int r = 0; r < R; ++r) it.store(base + r * 32 + lane, x[r]);
+    }
+}
+
+template <typename Items>
+__device__ void block_bitonic_sort(const Items& it, int n_pad) {
+    __syncthreads();
+    const int nw = blockDim.x >> 5;
+    const int ch = n_pad / nw;
+    if (ch * nw == n_pad && ch >= 32 && ch <= 256) {
+        if (ch == 32) bitonic_sort_chunks<1>(it, n_pad);
+        else if (ch == 64) bitonic_sort_chunks<2>(it, n_pad);
+        else if (ch == 128) bitonic_sort_chunks<4>(it, n_pad);
+        else bitonic_sort_chunks<8>(it, n_pad);
+    } else {
+        for (int k = 2; k <= n_pad; k <<= 1)
+            for (int jj = k >> 1; jj > 0; jj >>= 1) {
+                bitonic_smem_stage(it, n_pad, k, jj);
+                __syncthreads();
+            }
+    }
+    __syncthreads();
+}
+
+// In-place sort of (w, key, r) by merge_before over n_pad (power of 2) slots.
+template <typename T>
+__device__ void sort_survivors(T* s_w, uint32_t* s_key, int* s_r, int n_pad) {
+    block_bitonic_sort(SurvItems<T>{s_w, s_key, s_r}, n_pad);
 }
 
 // Block-wide exclusive scan of int flags; returns the total.  Starts with a barrier:
@@ -918,21 +1033,7 @@ __device__ uint64_t select_kth_largest(const T* w, int n, int k, int* s_tmp) {
 
 // In-place bitonic sort of (key, payload) ascending by key over n_pad (power of 2) slots.
 __device__ void sort_keys(uint32_t* key, int* val, int n_pad) {
-    for (int k = 2; k <= n_pad; k <<= 1) {
-        for (int jj = k >> 1; jj > 0; jj >>= 1) {
-            for (int i = threadIdx.x; i < n_pad; i += blockDim.x) {
-                int ixj = i ^ jj;
-                if (ixj > i) {
-                    bool up = (i & k) == 0;
-                    if ((key[i] > key[ixj]) == up) {
-                        uint32_t tk = key[i]; key[i] = key[ixj]; key[ixj] = tk;
-                        int tv = val[i]; val[i] = val[ixj]; val[ixj] = tv;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    }
+    block_bitonic_sort(KeyItems{key, val}, n_pad);
 }
 
 // Greedy reduction of phdUpdateMergeKernel (src/kernels.cu:693-866) over n
