@@ -1014,14 +1014,31 @@ __device__ uint64_t select_kth_largest(const T* w, int n, int k, int* s_tmp) {
             if ((key & mask) == prefix) atomicAdd(&s_hist[(key >> (8 * d)) & 255], 1);
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            int kk = s_k, b = 255;
-            for (; b > 0; --b) {
-                if (s_hist[b] >= kk) break;
-                kk -= s_hist[b];
+        if (threadIdx.x < 32) {
+            // the bin holding the k-th largest: counts from the top bin down, lane l owning
+            // bins 255-8l .. 248-8l; the first lane whose running total reaches k walks its 8
+            const int lane = threadIdx.x;
+            int c[8], sum = 0;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) { c[q] = s_hist[255 - 8 * lane - q]; sum += c[q]; }
+            int incl = sum;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
             }
-            s_k = kk;
-            s_prefix = prefix | ((uint64_t)b << (8 * d));
+            const int kk = s_k;
+            const unsigned hit = __ballot_sync(0xffffffffu, incl >= kk);
+            const int owner = hit ? __ffs(hit) - 1 : 31;
+            if (lane == owner) {
+                int rem = kk - (incl - sum), b = 255 - 8 * lane;
+                for (int q = 0; q < 8; ++q, --b) {
+                    if (b == 0 || c[q] >= rem) break;
+                    rem -= c[q];
+                }
+                s_k = rem;
+                s_prefix = prefix | ((uint64_t)b << (8 * d));
+            }
         }
         __syncthreads();
         prefix = s_prefix;
@@ -1367,11 +1384,11 @@ __device__ __forceinline__ void merge_body(const Params& prm, const Bufs<T>& b, 
     __syncthreads();
     const int n_out = block_exclusive_scan(s_pos, n, s_tmp);
     T* out = b.merged + (size_t)p * prm.Scap * kRow;
-    for (int i = tid; i < n; i += blockDim.x) {
-        if (i < stop && ms.is_center[i]) {
-            const T* sr = sparse + (size_t)i * kRow;
-            T* dr = out + (size_t)s_pos[i] * kRow;
-            for (int q = 0; q < 28; ++q) dr[q] = sr[q];
+    {   // centre rows in output order, one warp per row, lane q copying value q
+        const int lane = tid & 31;
+        for (int i = tid >> 5; i < n; i += blockDim.x >> 5) {
+            if (i < stop && ms.is_center[i] && lane < 28)
+                out[(size_t)s_pos[i] * kRow + lane] = sparse[(size_t)i * kRow + lane];
         }
     }
     __syncthreads();
