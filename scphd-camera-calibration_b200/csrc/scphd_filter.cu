@@ -202,7 +202,7 @@ public:
         b.surv_r = a.take<int>(N * S);
         b.surv_w = a.take<T>(N * S);
         b.surv_n = a.take<int>(N);
-        b.merged = a.take<T>(N * S * kRow);
+        b.mlist = a.take<int>(N * S);
         b.mtmp = a.take<T>(N * S * kRow);
         b.merged_n = a.take<int>(N);
         b.loglik = a.take<double>(N);
@@ -411,9 +411,23 @@ public:
             base = b.fit + (size_t)p * prm.Gcap * kRow;
             width = 29;
         } else if (which == SCPHD_MIX_MERGED) {
+            // merged rows stay where the merge wrote them, listed in output order
             CUDA_TRY(cudaMemcpyAsync(&cnt, b.merged_n + p, sizeof(int), cudaMemcpyDeviceToHost, stream));
-            base = b.merged + (size_t)p * prm.Scap * kRow;
-            width = 28;
+            CUDA_TRY(cudaStreamSynchronize(stream));
+            if (count) *count = cnt;
+            if (!out || cnt == 0) return SCPHD_OK;
+            std::vector<int> list(cnt);
+            std::vector<T> rows((size_t)prm.Scap * kRow);
+            CUDA_TRY(cudaMemcpyAsync(list.data(), b.mlist + (size_t)p * prm.Scap, sizeof(int) * cnt,
+                                     cudaMemcpyDeviceToHost, stream));
+            CUDA_TRY(cudaMemcpyAsync(rows.data(), b.mtmp + (size_t)p * prm.Scap * kRow, sizeof(T) * rows.size(),
+                                     cudaMemcpyDeviceToHost, stream));
+            CUDA_TRY(cudaStreamSynchronize(stream));
+            for (int i = 0; i < cnt; ++i) {
+                if (list[i] < 0 || list[i] >= prm.Scap) return fail(SCPHD_ERR_INVALID, "corrupt merged list");
+                for (int q = 0; q < 28; ++q) out[(size_t)i * 28 + q] = (double)rows[(size_t)list[i] * kRow + q];
+            }
+            return SCPHD_OK;
         } else {
             return fail(SCPHD_ERR_INVALID, "unknown mixture selector");
         }

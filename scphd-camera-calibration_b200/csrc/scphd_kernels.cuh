@@ -50,7 +50,7 @@ template <typename T> struct Bufs {
     int* surv_r;        // N x Scap survivor ranks
     T* surv_w;          // N x Scap survivor weights
     int* surv_n;        // N
-    T* merged;          // N x Scap rows of kRow (merge output, in order)
+    int* mlist;         // N x Scap: centre index of each merged component, in output order
     T* mtmp;            // N x Scap rows of kRow (merge output indexed by centre)
     int* merged_n;      // N
     double* loglik;     // N
@@ -1383,15 +1383,13 @@ __device__ __forceinline__ void merge_body(const Params& prm, const Bufs<T>& b, 
     for (int i = tid; i < n; i += blockDim.x) s_pos[i] = (i < stop && ms.is_center[i]) ? 1 : 0;
     __syncthreads();
     const int n_out = block_exclusive_scan(s_pos, n, s_tmp);
-    T* out = b.merged + (size_t)p * prm.Scap * kRow;
-    {   // centre rows in output order, one warp per row, lane q copying value q
-        const int lane = tid & 31;
-        for (int i = tid >> 5; i < n; i += blockDim.x >> 5) {
-            if (i < stop && ms.is_center[i] && lane < 28)
-                out[(size_t)s_pos[i] * kRow + lane] = sparse[(size_t)i * kRow + lane];
-        }
-    }
+    // merged component e (output order) is the row sparse[centre_of[e]]; the member
+    // lists are dead once the merge has run, so their slots hold centre_of
+    int* centre_of = ms.perm;
+    for (int i = tid; i < n; i += blockDim.x)
+        if (i < stop && ms.is_center[i]) centre_of[s_pos[i]] = i;
     __syncthreads();
+    for (int e = tid; e < n_out; e += blockDim.x) b.mlist[(size_t)p * prm.Scap + e] = centre_of[e];
     // new map: merged components then retained non-detection clouds (.cu:1923-2058);
     // entries e < n_out are merged, e >= n_out are the Gaussians j = e - n_out
     const T minw = (T)prm.min_weight;
@@ -1400,7 +1398,7 @@ __device__ __forceinline__ void merge_body(const Params& prm, const Bufs<T>& b, 
     for (int e = tid; e < n_all; e += blockDim.x) {
         T w;
         if (e < n_out) {
-            w = out[(size_t)e * kRow];
+            w = sparse[(size_t)centre_of[e] * kRow];
         } else {
             const T* fr = b.fit + ((size_t)p * prm.Gcap + (e - n_out)) * kRow;
             const T wnd = nd_weight(fr[0], fr[1]);
@@ -1453,7 +1451,7 @@ __device__ __forceinline__ void merge_body(const Params& prm, const Bufs<T>& b, 
         const int nxt = (e + 1 < n_all) ? s_pos[e + 1] : total;
         if (nxt == pos) continue;   // not kept
         if (e < n_out) {   // merged component: weight, mean and the Cholesky factor of its covariance
-            const T* sr = out + (size_t)e * kRow;
+            const T* sr = sparse + (size_t)centre_of[e] * kRow;
             T L[21];
             chol6(sr + 7, L);
             T* dr = mo + (size_t)pos * kRow;
