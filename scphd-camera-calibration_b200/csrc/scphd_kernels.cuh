@@ -634,6 +634,9 @@ __global__ void __launch_bounds__(1024)
 // Component sources for the merge loop: posterior components of one parent
 // (detections and births), or an explicit list.
 template <typename T, int K> struct KalmanSource {
+    // every component has a PD covariance (posteriors passed the PD test, births are
+    // diagonal), so a centre's distance to itself is exactly 0 < min_separation
+    static constexpr bool kSelfAbsorbs = true;
     const T* fit;   // parent's fitted rows
     const T* prep;  // parent's prep rows
     const T* z;     // measurements
@@ -672,6 +675,7 @@ template <typename T, int K> struct KalmanSource {
 };
 
 template <typename T> struct ListSource {
+    static constexpr bool kSelfAbsorbs = false;   // caller's rows: the self-distance is evaluated
     const T* rows;   // n rows of kRow
     __device__ void mean(int r, T mu[6]) const {
 #pragma unroll
@@ -949,7 +953,12 @@ __device__ void merge_members_thread(const Src& src, const T* s_w, const int* s_
     for (uint32_t mb = mbits; mb; mb &= mb - 1) {
         int i = mem[__ffs(mb) - 1];
         T w = s_w[i], mu[6];
-        src.mean(s_r[i], mu);
+        if (i == c) {   // the centre's mean is already at hand (same values)
+#pragma unroll
+            for (int a = 0; a < 6; ++a) mu[a] = cmu[a];
+        } else {
+            src.mean(s_r[i], mu);
+        }
         W += w;
 #pragma unroll
         for (int a = 0; a < 6; ++a) acc[a] += w * mu[a];
@@ -964,7 +973,12 @@ __device__ void merge_members_thread(const Src& src, const T* s_w, const int* s_
     for (uint32_t mb = mbits; mb; mb &= mb - 1) {
         int i = mem[__ffs(mb) - 1];
         T w = s_w[i], mu[6], d[6];
-        src.mean(s_r[i], mu);
+        if (i == c) {
+#pragma unroll
+            for (int a = 0; a < 6; ++a) mu[a] = cmu[a];
+        } else {
+            src.mean(s_r[i], mu);
+        }
         const T* sc = src.cov(s_r[i]);
 #pragma unroll
         for (int a = 0; a < 6; ++a) d[a] = row[1 + a] - mu[a];
@@ -1189,6 +1203,10 @@ __device__ int merge_components(const Src& src, const T* s_w, const int* s_r, in
             for (int k = k0; k < cnt; ++k) {
                 if ((done >> k) & 1u) continue;
                 const int i = mem[k];
+                if (Src::kSelfAbsorbs && k == k0) {   // distance to itself: 0
+                    mbits |= 1u << k;
+                    continue;
+                }
                 if (!could_merge_f(ms.pf + cc * 6, ms.pf + i * 6, fsep, fmargin)) continue;
                 ++evals;
                 T mu[6];
