@@ -234,7 +234,10 @@ public:
         carve(a);
         CUDA_TRY(cudaMemsetAsync(p, 0, probe.used, stream));
         merge_smem = merge_smem_bytes<T>(prm.Scap, prm.Gcap, 4);
-        fit_smem = cloud_fit_smem_bytes<T>(prm.Ps);
+        fit_smem = cloud_fit_smem_bytes<T>(prm.P);
+        if (fit_smem > 220 * 1024)   // with the kernel's static shared memory, within 227 KB per block
+            return fail(SCPHD_ERR_CAPACITY, "particles_per_feature needs " + std::to_string(fit_smem) +
+                                                " bytes of shared memory per cloud-fit block (FP64 allows up to 212)");
         if (merge_smem > 227 * 1024)
             return fail(SCPHD_ERR_CAPACITY, "max_survivors/max_gaussians need " + std::to_string(merge_smem) +
                                                 " bytes of shared memory per merge block (limit 227 KB)");
@@ -1120,7 +1123,7 @@ template <typename T> struct Batch final : scphd_batch {
                 stage_off[first + i] = stage_total;
                 stage_total += 3 * (size_t)pr.Mcap;
                 merge_smem = std::max(merge_smem, merge_smem_bytes<T>(pr.Scap, pr.Gcap, 4));
-                fit_smem = std::max(fit_smem, cloud_fit_smem_bytes<T>(pr.Ps));
+                fit_smem = std::max(fit_smem, cloud_fit_smem_bytes<T>(pr.P));
                 lik_smem = std::max(lik_smem, likelihood_smem_bytes<T>(pr.Gcap));
             }
             g.n_parent = (int)mp.back().size();

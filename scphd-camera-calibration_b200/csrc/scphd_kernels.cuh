@@ -223,18 +223,21 @@ __device__ __forceinline__ double moment_sweep(const double* w, const double* a,
     return (s0 + s1) + (s2 + s3);
 }
 
-// Row stride of the staged samples, in elements: at least Ps, a multiple of 16 bytes,
-// and 12 words modulo 32 banks, so that the eight rows a lane-per-moment sweep reads
-// at one sample index fall in distinct banks.
-template <typename T> __host__ __device__ inline int stage_stride(int Ps) {
-    if (sizeof(T) == 4) return Ps + (((12 - Ps) % 32) + 32) % 32;
-    return Ps + (((6 - Ps) % 16) + 16) % 16;
+// Staged sample rows: each warp works on Gaussians in pairs and stages, per Gaussian of
+// the pair, 8 rows of P4 = round_up(P, 4) values: the samples' (u, v, d, vu, vv, vd),
+// their weights w', and ones.  The row stride is P4 or the next size whose rows start
+// an odd multiple of 4 banks apart, so that the eight rows a lane-per-moment sweep reads
+// at one sample index (16-byte pieces) fall in distinct banks.
+template <typename T> __host__ __device__ inline int stage_stride(int P4) {
+    if (sizeof(T) == 4) return (P4 % 8 == 4) ? P4 : P4 + 4;
+    return P4 + 2;
 }
 constexpr int kFitWarps = 8;
-constexpr int kStageRows = 8;   // d[6], w', ones
-template <typename T> __host__ __device__ inline size_t cloud_fit_smem_bytes(int Ps) {
-    const size_t stage = (size_t)kFitWarps * kStageRows * stage_stride<T>(Ps);   // sample rows
-    const size_t prep = (size_t)kFitWarps * 32 * 42;                             // per-thread Kalman scratch
+constexpr int kStageRows = 8;   // y[6], w', ones
+template <typename T> __host__ __device__ inline size_t cloud_fit_smem_bytes(int P) {
+    const int P4 = (P + 3) & ~3;
+    const size_t stage = (size_t)kFitWarps * 2 * kStageRows * stage_stride<T>(P4);   // sample rows
+    const size_t prep = (size_t)kFitWarps * 32 * 42;                                  // per-thread Kalman scratch
     return (stage > prep ? stage : prep) * sizeof(T);
 }
 
@@ -254,11 +257,12 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
     const int row = b.src[p];
     const int G = min(b.map_n[cur][row], prm.Gcap);
     const int P = prm.P, Ps = prm.Ps;
-    const int sY = stage_stride<T>(Ps);
-    T* Y = s_stage + (size_t)warp * kStageRows * sY;   // rows 0-5 d, 6 w', 7 ones
+    const int P4 = (P + 3) & ~3;
+    const int sY = stage_stride<T>(P4);
+    T* Ywarp = s_stage + (size_t)warp * 2 * kStageRows * sY;   // per Gaussian of the pair: y[6], w', ones
     __shared__ Pose<T> pose_upd, pose_src;
     __shared__ int s_rd, s_wr;
-    __shared__ __align__(16) T s_L[kFitWarps * 28];   // per warp: Cholesky factor and mean of a merged component
+    __shared__ __align__(16) T s_L[kFitWarps * 2 * 28];   // per warp and Gaussian: Cholesky factor and mean
     __shared__ T s_fit[kFitWarps * 32];  // per warp: the fitted row (W, pD, mean[6], cov[21])
     if (threadIdx.x == 0) {
         double zero[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -270,12 +274,14 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
         s_rd = 0;
         s_wr = 0;
     }
-    for (int s = lane; s < sY; s += 32) Y[7 * sY + s] = T(1);
+    for (int s = lane; s < sY; s += 32) {
+        Ywarp[7 * sY + s] = T(1);
+        Ywarp[(kStageRows + 7) * sY + s] = T(1);
+    }
     __syncthreads();
     const Model& m = prm.model;
     const T invP = T(1) / T(P);
     const T dtT = (T)dt, half_dt2 = T(0.5) * (T)dt * (T)dt;
-    T* Lw = s_L + warp * 28;
     T* fitw = s_fit + warp * 32;
     // moment owned by this lane: rows (ra, rb) of the weighted product w' * Y[ra] * Y[rb]
     int ra = 7, rb = 7;
@@ -287,33 +293,43 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
         ra = aa;
         rb = e - aa * (aa + 1) / 2;
     }
-    const int P4 = (P + 3) & ~3;
-    for (int j = warp; j < G; j += kFitWarps) {
-        const size_t erow = (size_t)row * prm.Gcap + j;
-        const T* ent = b.map[cur] + erow * kRow;
-        const int ref = b.map_ref[cur][erow];
-        const T W = has_pred ? ent[0] * (T)prm.ps : ent[0];
-        const T* cl_in = ref >= 0 ? b.cloud[cur] + (size_t)ref * 7 * Ps : nullptr;
-        if (ref < 0) {   // Cholesky factor (21, stored in the map row) and mean (6) of the merged component
-            if (lane < 21) Lw[lane] = ent[7 + lane];
-            else if (lane < 27) Lw[lane] = ent[1 + lane - 21];
-            else if (lane == 27) Lw[27] = T(0);
-        } else if (lane == 0) {
-            atomicAdd(&s_rd, 1);
+    for (int j0 = 2 * warp; j0 < G; j0 += 2 * kFitWarps) {
+        const int nG = min(2, G - j0);
+        // the pair's entries (map order keeps merged components first, so a pair is
+        // nearly always of one kind and the sample loop does not diverge)
+        int refg[2] = {0, 0};
+        T Wg[2] = {T(0), T(0)};
+        for (int g = 0; g < nG; ++g) {
+            const size_t erow = (size_t)row * prm.Gcap + j0 + g;
+            const T* ent = b.map[cur] + erow * kRow;
+            const int ref = b.map_ref[cur][erow];
+            refg[g] = ref;
+            Wg[g] = has_pred ? ent[0] * (T)prm.ps : ent[0];
+            T* Lw = s_L + (warp * 2 + g) * 28;
+            if (ref < 0) {   // Cholesky factor (21, stored in the map row) and mean (6) of the merged component
+                if (lane < 21) Lw[lane] = ent[7 + lane];
+                else if (lane < 27) Lw[lane] = ent[1 + lane - 21];
+                else if (lane == 27) Lw[27] = T(0);
+            } else if (lane == 0) {
+                atomicAdd(&s_rd, 1);
+            }
         }
         __syncwarp();
-        const bool write_nd = W >= (T)prm.min_weight;
-        T* cl_out = b.cloud[cur ^ 1] + ((size_t)p * prm.Gcap + j) * 7 * Ps;
-        const uint32_t key_i = (uint32_t)(-1 - ref);
-        T shift[6];
-        int n_in = 0;
-        bool any_w = false;
-        for (int t = 0; t * 32 < P; ++t) {
-            const int s = lane + 32 * t;
-            const bool valid = s < P;
+        const bool wnd0 = Wg[0] >= (T)prm.min_weight, wnd1 = Wg[1] >= (T)prm.min_weight;
+        const int total = nG * P;
+        int n_in0 = 0, n_in1 = 0;
+        bool any0 = false, any1 = false;
+        for (int t = 0; t * 32 < total; ++t) {
+            const int f = lane + 32 * t;
+            const bool valid = f < total;
+            const int g = f >= P ? 1 : 0;
+            const int s = f - g * P;
+            const int ref = g ? refg[1] : refg[0];
+            const int j = j0 + g;
             T X[6], om = 0, y[6];
             if (valid) {
                 if (ref < 0) {   // merged component: draw (.cu:640-690) and map to world (.cu:1222-1286)
+                    const uint32_t key_i = (uint32_t)(-1 - ref);
                     uint32_t w0[4], w1[4];
                     philox((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 0), prm.key0,
                            prm.key1, w0);
@@ -324,10 +340,11 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
                     Pair<T>::two(w0[2], w0[3], z[2], z[3]);
                     Pair<T>::two(w1[0], w1[1], z[4], z[5]);
                     T yy[6];
-                    ltz_plus_mean(Lw, z, yy);   // y = L z + mean from the warp's shared line
+                    ltz_plus_mean(s_L + (warp * 2 + g) * 28, z, yy);   // y = L z + mean
                     invert(yy, pose_src, m, X);
                     om = invP;
                 } else {         // non-detection cloud carried from the previous frame
+                    const T* cl_in = b.cloud[cur] + (size_t)ref * 7 * Ps;
 #pragma unroll
                     for (int a2 = 0; a2 < 6; ++a2) X[a2] = cl_in[a2 * Ps + s];
                     om = cl_in[6 * Ps + s];
@@ -353,91 +370,104 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
             }
             const bool inr = valid && in_range(y, m);
             const T pds = inr ? (T)m.pd : T(0);
-            n_in += __popc(__ballot_sync(0xffffffffu, inr));
-            if (t == 0) {   // shift: the warp's first sample (finite), else 0
-#pragma unroll
-                for (int a2 = 0; a2 < 6; ++a2) {
-                    T v = __shfl_sync(0xffffffffu, y[a2], 0);
-                    shift[a2] = isfinite(v) ? v : T(0);
-                }
-            }
-            if (valid && write_nd) {   // non-detection cloud candidate: predicted world point, weight 1 - pD
+            const unsigned in_mask = __ballot_sync(0xffffffffu, inr);
+            const unsigned g_mask = __ballot_sync(0xffffffffu, valid && g == 1);
+            n_in0 += __popc(in_mask & ~g_mask);
+            n_in1 += __popc(in_mask & g_mask);
+            if (valid && (g ? wnd1 : wnd0)) {   // non-detection cloud candidate: predicted world point, weight 1 - pD
+                T* cl_out = b.cloud[cur ^ 1] + ((size_t)p * prm.Gcap + j) * 7 * Ps;
 #pragma unroll
                 for (int a2 = 0; a2 < 6; ++a2) __stcs(cl_out + a2 * Ps + s, X[a2]);
                 __stcs(cl_out + 6 * Ps + s, T(1) - pds);
             }
             const T wp = om * pds;
-            any_w |= wp != T(0);
-            if (s < sY) {
+            if (g) any1 |= wp != T(0);
+            else any0 |= wp != T(0);
+            if (valid) {   // staged as measured; the shift is taken per Gaussian below
+                T* Y = Ywarp + (size_t)g * kStageRows * sY;
 #pragma unroll
-                for (int a2 = 0; a2 < 6; ++a2) Y[a2 * sY + s] = valid ? y[a2] - shift[a2] : T(0);
+                for (int a2 = 0; a2 < 6; ++a2) Y[a2 * sY + s] = y[a2];
                 Y[6 * sY + s] = wp;
             }
         }
-        if (write_nd && lane == 0) atomicAdd(&s_wr, 1);
+        if (lane == 0) atomicAdd(&s_wr, (int)wnd0 + (nG > 1 ? (int)wnd1 : 0));
+        any0 = __any_sync(0xffffffffu, any0);
+        any1 = __any_sync(0xffffffffu, any1);
         __syncwarp();
-        any_w = __any_sync(0xffffffffu, any_w);
-        const T pbar = (T)((double)n_in * m.pd / (double)P);
-        if (any_w) {
-            // zero-weight samples leave the sums (their d may be non-finite)
-            for (int s = lane; s < P; s += 32)
-                if (Y[6 * sY + s] == T(0)) {
-#pragma unroll
-                    for (int a2 = 0; a2 < 6; ++a2) Y[a2 * sY + s] = T(0);
-                }
-            __syncwarp();
-            // lane q < 29: moment q over the samples, four partial sums
-            const T mom = lane < 29 ? moment_sweep(Y + 6 * sY, Y + ra * sY, Y + rb * sY, P4) : T(0);
-            const T S0 = __shfl_sync(0xffffffffu, mom, 0), S2 = __shfl_sync(0xffffffffu, mom, 1);
-            const T inv = T(1) / S0, scale = T(1) + S2 * inv * inv;
-            // lanes 2-7 hold S1 (the mean offsets), lanes 8-28 hold SS
-            const T dl = (lane >= 2 && lane < 8) ? mom * inv : T(0);
-            T da = 0, db = 0;
-            T dvals[6];
-#pragma unroll
-            for (int a2 = 0; a2 < 6; ++a2) dvals[a2] = __shfl_sync(0xffffffffu, dl, 2 + a2);
+        for (int g = 0; g < nG; ++g) {
+            const int j = j0 + g;
+            const T W = g ? Wg[1] : Wg[0];
+            T* Y = Ywarp + (size_t)g * kStageRows * sY;
+            const bool any_w = g ? any1 : any0;
+            const T pbar = (T)((double)(g ? n_in1 : n_in0) * m.pd / (double)P);
+            T shift[6];   // the Gaussian's first sample, if finite, else 0
 #pragma unroll
             for (int a2 = 0; a2 < 6; ++a2) {
-                if (ra == a2) da = dvals[a2];
-                if (rb == a2) db = dvals[a2];
+                const T v = Y[a2 * sY];
+                shift[a2] = isfinite(v) ? v : T(0);
             }
-            if (lane >= 2 && lane < 8) fitw[lane] = shift[lane - 2] + dl;
-            if (lane >= 8 && lane < 29) fitw[lane] = (mom * inv - da * db) * scale;
-        } else if (pbar > T(0)) {
-            // every sample weighted 1 (exp(LOG0 - LOG0)): unnormalised mean (sum of the
-            // samples) and covariance x (P + P)/P over the valid samples
-            T mu = 0;
-            if (lane < 6) {
-                for (int s = 0; s < P; ++s) mu += Y[lane * sY + s] + shift[lane];
-            }
-            T mus[6];
+            __syncwarp();
+            if (any_w) {
+                // d = y - shift; zero-weight samples (and the padding) leave the sums
+                for (int s = lane; s < P4; s += 32) {
+                    const T w = s < P ? Y[6 * sY + s] : T(0);
 #pragma unroll
-            for (int a2 = 0; a2 < 6; ++a2) mus[a2] = __shfl_sync(0xffffffffu, mu, a2);
-            T cva = 0;
-            if (lane >= 8 && lane < 29) {
-                T ma = 0, mb = 0, sa = 0, sb = 0;
+                    for (int a2 = 0; a2 < 6; ++a2) Y[a2 * sY + s] = w != T(0) ? Y[a2 * sY + s] - shift[a2] : T(0);
+                    if (s >= P) Y[6 * sY + s] = T(0);
+                }
+                __syncwarp();
+                // lane q < 29: moment q over the samples, four partial sums
+                const T mom = lane < 29 ? moment_sweep(Y + 6 * sY, Y + ra * sY, Y + rb * sY, P4) : T(0);
+                const T S0 = __shfl_sync(0xffffffffu, mom, 0), S2 = __shfl_sync(0xffffffffu, mom, 1);
+                const T inv = T(1) / S0, scale = T(1) + S2 * inv * inv;
+                // lanes 2-7 hold S1 (the mean offsets), lanes 8-28 hold SS
+                const T dl = (lane >= 2 && lane < 8) ? mom * inv : T(0);
+                T da = 0, db = 0;
+                T dvals[6];
+#pragma unroll
+                for (int a2 = 0; a2 < 6; ++a2) dvals[a2] = __shfl_sync(0xffffffffu, dl, 2 + a2);
 #pragma unroll
                 for (int a2 = 0; a2 < 6; ++a2) {
-                    if (ra == a2) { ma = mus[a2]; sa = shift[a2]; }
-                    if (rb == a2) { mb = mus[a2]; sb = shift[a2]; }
+                    if (ra == a2) da = dvals[a2];
+                    if (rb == a2) db = dvals[a2];
                 }
-                for (int s = 0; s < P; ++s)
-                    cva += ((Y[ra * sY + s] + sa) - ma) * ((Y[rb * sY + s] + sb) - mb);
+                if (lane >= 2 && lane < 8) fitw[lane] = shift[lane - 2] + dl;
+                if (lane >= 8 && lane < 29) fitw[lane] = (mom * inv - da * db) * scale;
+            } else if (pbar > T(0)) {
+                // every sample weighted 1 (exp(LOG0 - LOG0)): unnormalised mean (sum of the
+                // samples) and covariance x (P + P)/P over the valid samples
+                T mu = 0;
+                if (lane < 6) {
+                    for (int s = 0; s < P; ++s) mu += Y[lane * sY + s];
+                }
+                T mus[6];
+#pragma unroll
+                for (int a2 = 0; a2 < 6; ++a2) mus[a2] = __shfl_sync(0xffffffffu, mu, a2);
+                T cva = 0;
+                if (lane >= 8 && lane < 29) {
+                    T ma = 0, mb = 0;
+#pragma unroll
+                    for (int a2 = 0; a2 < 6; ++a2) {
+                        if (ra == a2) ma = mus[a2];
+                        if (rb == a2) mb = mus[a2];
+                    }
+                    for (int s = 0; s < P; ++s) cva += (Y[ra * sY + s] - ma) * (Y[rb * sY + s] - mb);
+                }
+                const T scale = (T(P) * T(P) + T(P)) / T(P);
+                if (lane < 6) fitw[2 + lane] = mu;
+                if (lane >= 8 && lane < 29) fitw[lane] = cva * scale;
+            } else {   // entirely out of view: never used downstream (its log-constant is -inf)
+                if (lane < 6) fitw[2 + lane] = shift[lane];
+                if (lane >= 8 && lane < 29) fitw[lane] = T(0);
             }
-            const T scale = (T(P) * T(P) + T(P)) / T(P);
-            if (lane < 6) fitw[2 + lane] = mu;
-            if (lane >= 8 && lane < 29) fitw[lane] = cva * scale;
-        } else {   // entirely out of view: never used downstream (its log-constant is -inf)
-            if (lane < 6) fitw[2 + lane] = shift[lane];
-            if (lane >= 8 && lane < 29) fitw[lane] = T(0);
+            if (lane == 0) fitw[0] = W;
+            if (lane == 1) fitw[1] = pbar;
+            __syncwarp();
+            // fitted row: lane q writes element q (W, pD, mean[6], packed cov[21])
+            T* fr = b.fit + ((size_t)p * prm.Gcap + j) * kRow;
+            if (lane < 29) fr[lane] = fitw[lane];
+            __syncwarp();
         }
-        if (lane == 0) fitw[0] = W;
-        if (lane == 1) fitw[1] = pbar;
-        __syncwarp();
-        // fitted row: lane q writes element q (W, pD, mean[6], packed cov[21])
-        T* fr = b.fit + ((size_t)p * prm.Gcap + j) * kRow;
-        if (lane < 29) fr[lane] = fitw[lane];
-        __syncwarp();
     }
     __syncthreads();
     // measurement-independent Kalman terms, one thread per fitted Gaussian; the fitted
