@@ -303,7 +303,7 @@ public:
             const int bs = likelihood_block(M);
             dim3 grid(N, (M + bs - 1) / bs);
             h = stage_begin(2);
-            k_likelihood<T, K><<<grid, bs, likelihood_smem_bytes<T>(prm.Gcap), stream>>>(prm, b, cur, M);
+            k_likelihood<T, K><<<grid, bs, likelihood_smem_bytes<T>(prm.Gcap, bs), stream>>>(prm, b, cur, M);
             LAUNCHED();
             stage_end(h);
         }
@@ -1124,7 +1124,7 @@ template <typename T> struct Batch final : scphd_batch {
                 stage_total += 3 * (size_t)pr.Mcap;
                 merge_smem = std::max(merge_smem, merge_smem_bytes<T>(pr.Scap, pr.Gcap, 4));
                 fit_smem = std::max(fit_smem, cloud_fit_smem_bytes<T>(pr.P));
-                lik_smem = std::max(lik_smem, likelihood_smem_bytes<T>(pr.Gcap));
+                lik_smem = std::max(lik_smem, likelihood_smem_bytes<T>(pr.Gcap, lik_block));
             }
             g.n_parent = (int)mp.back().size();
             g.n_pred = (int)mpred.back().size();

@@ -516,10 +516,15 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
 // with a PD posterior (updateKernel, kernels.cu:622-657), births likewise.
 // One thread per measurement; a block covers the frame's measurements (a multiple
 // of 32 threads, up to 1024; more measurements take more blocks) and stages the
-// parent's Gaussian terms once in shared memory for both passes.
+// parent's Gaussian terms once in shared memory for both passes.  Since ell >= bpc =
+// log(M w0 + kappa) (the sum inside the log holds exp(0) = 1 around its larger term),
+// a pair with log w < bpc + log(min_weight) - 1 can never reach min_weight; the first
+// pass remembers the pairs above that bound (up to kLikCand per measurement) and the
+// survivor pass evaluates only those (all pairs again if the list overflowed).
 constexpr int kLikTerms = 12;   // log-constant, PD flag, S^-1 (6), mean (3), pad: 16-byte pieces
-template <typename T> __host__ __device__ inline size_t likelihood_smem_bytes(int Gcap) {
-    return (size_t)Gcap * kLikTerms * sizeof(T);
+constexpr int kLikCand = 16;   // candidate survivors remembered per measurement
+template <typename T> __host__ __device__ inline size_t likelihood_smem_bytes(int Gcap, int block) {
+    return (size_t)Gcap * kLikTerms * sizeof(T) + (size_t)block * kLikCand * sizeof(int);
 }
 __host__ __device__ inline int likelihood_block(int M) {
     const int r = (M + 31) / 32 * 32;
@@ -566,6 +571,9 @@ __device__ __forceinline__ void likelihood_body(const Params& prm, const Bufs<T>
         for (int a2 = 0; a2 < K; ++a2) zm[a2] = b.z[m * 3 + a2];
     }
     const T bpc = (T)log((double)M * prm.w0 + prm.kappa);
+    const T cand_min = bpc + (T)log(prm.min_weight) - T(1);
+    int* s_cand = reinterpret_cast<int*>(s_terms + (size_t)prm.Gcap * kLikTerms);   // [slot][thread]
+    int n_cand = 0;
     __syncthreads();
     T mx = tneg_inf<T>(), acc = 0;
     if (m < M) {
@@ -578,6 +586,10 @@ __device__ __forceinline__ void likelihood_body(const Params& prm, const Bufs<T>
             const T lt = log_term<T, K>(c, t + 2, t + 8, zm);
             if (lt > mx) { acc = acc * texp(mx - lt) + T(1); mx = lt; }   // online log-sum-exp
             else acc += texp(lt - mx);
+            if (lt >= cand_min) {
+                if (n_cand < kLikCand) s_cand[n_cand * blockDim.x + threadIdx.x] = k;
+                ++n_cand;
+            }
         }
     }
     T ell = bpc;
@@ -587,28 +599,21 @@ __device__ __forceinline__ void likelihood_body(const Params& prm, const Bufs<T>
         ell = big + tlog(acc * texp(mx - big) + texp(bpc - big));
     }
     if (m < M) b.ell[(size_t)p * prm.Mcap + m] = ell;
-    // survivors
+    // survivors among the candidates (or all pairs, if the list overflowed)
     const T minw = (T)prm.min_weight;
     const unsigned lane = threadIdx.x & 31;
-    for (int k = 0; k < G; ++k) {
-        bool keep = false;
-        T w = 0;
-        if (m < M) {
+    if (m < M) {
+        const bool all = n_cand > kLikCand;
+        const int nk = all ? G : n_cand;
+        for (int q = 0; q < nk; ++q) {
+            const int k = all ? q : s_cand[q * blockDim.x + threadIdx.x];
             T t[kLikTerms];
             load_terms(s_terms + (size_t)k * kLikTerms, t);
             const T c = t[0];
-            if (c > tneg_inf<T>() && t[1] > T(0)) {
-                w = texp(log_term<T, K>(c, t + 2, t + 8, zm) - ell);
-                keep = w >= minw;
-            }
-        }
-        unsigned mask = __ballot_sync(0xffffffffu, keep);
-        if (mask) {
-            int base = 0;
-            if (lane == 0) base = atomicAdd(&b.surv_n[p], __popc(mask));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (keep) {
-                int slot = base + __popc(mask & ((1u << lane) - 1u));
+            if (!(c > tneg_inf<T>() && t[1] > T(0))) continue;
+            const T w = texp(log_term<T, K>(c, t + 2, t + 8, zm) - ell);
+            if (w >= minw) {
+                const int slot = atomicAdd(&b.surv_n[p], 1);
                 if (slot < prm.Scap) {
                     b.surv_r[(size_t)p * prm.Scap + slot] = m * G + k;
                     b.surv_w[(size_t)p * prm.Scap + slot] = w;
