@@ -344,10 +344,12 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
                     invert(yy, pose_src, m, X);
                     om = invP;
                 } else {         // non-detection cloud carried from the previous frame
+                    // the previous frame's clouds are only read in this kernel (writes go to
+                    // the other buffer): read-only loads, free to move ahead of the stores
                     const T* cl_in = b.cloud[cur] + (size_t)ref * 7 * Ps;
 #pragma unroll
-                    for (int a2 = 0; a2 < 6; ++a2) X[a2] = cl_in[a2 * Ps + s];
-                    om = cl_in[6 * Ps + s];
+                    for (int a2 = 0; a2 < 6; ++a2) X[a2] = __ldg(cl_in + a2 * Ps + s);
+                    om = __ldg(cl_in + 6 * Ps + s);
                 }
                 if (has_pred) {   // predict_features with feature noise
                     uint32_t w[4];
