@@ -47,6 +47,21 @@ __host__ __device__ inline void philox(uint32_t c0, uint32_t c1, uint32_t c2, ui
     out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
 }
 
+// The same generator with its round keys taken from a table (rk[2r], rk[2r+1] = the
+// keys of round r): with the table in kernel parameters the keys cost no instructions.
+__device__ __forceinline__ void philox_rk(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, const uint32_t* rk,
+                                          uint32_t out[4]) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        const uint32_t n0 = hi1 ^ c1 ^ rk[2 * r], n2 = hi0 ^ c3 ^ rk[2 * r + 1];
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
 __host__ __device__ inline double u01(uint32_t w) { return ((double)w + 0.5) * 0x1p-32; }
 
 // four standard normals (two Box-Muller pairs) from one Philox block

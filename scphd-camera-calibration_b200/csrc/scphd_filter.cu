@@ -556,6 +556,10 @@ Params make_params(const scphd_config& c) {
     for (int i = 0; i < 12; ++i) { p.prior_a[i] = c.prior_a[i]; p.prior_b[i] = c.prior_b[i]; }
     p.key0 = (uint32_t)c.seed;
     p.key1 = (uint32_t)(c.seed >> 32);
+    for (int r = 0; r < 10; ++r) {   // Philox round keys
+        p.rk[2 * r] = p.key0 + 0x9E3779B9u * (uint32_t)r;
+        p.rk[2 * r + 1] = p.key1 + 0xBB67AE85u * (uint32_t)r;
+    }
     return p;
 }
 

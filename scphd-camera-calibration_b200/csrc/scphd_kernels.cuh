@@ -30,6 +30,7 @@ struct Params {
     double cam_std[6], feat_std[3];
     double prior_a[12], prior_b[12];
     uint32_t key0, key1;
+    uint32_t rk[20];   // Philox round keys (key0 + r C0, key1 + r C1), precomputed on the host
 };
 
 template <typename T> struct Bufs {
@@ -74,13 +75,15 @@ struct FrameArgs {
 
 // Up to kBatchSlots filters of a batch per launch: their constants and buffers as
 // one kernel parameter (read-only parameter space, like a single filter's Params;
-// 32 x 744 bytes fits the 32 KB parameter limit).  Each frame's per-filter
+// 32 x 824 bytes fits the 32 KB parameter limit).  Each frame's per-filter
 // arguments are a separate FrameArgs array in global memory.
 constexpr int kBatchSlots = 32;
 template <typename T> struct SlotTable {
     Params prm[kBatchSlots];
     Bufs<T> b[kBatchSlots];
 };
+// kernel parameters are limited to 32764 bytes: the table plus two pointers must fit
+static_assert(sizeof(SlotTable<double>) + 64 <= 32764, "batch parameter table exceeds the kernel parameter limit");
 
 __device__ __forceinline__ uint32_t tie_key(uint32_t r) {
     // argmax order of phdUpdateMergeKernel (src/kernels.cu:704-739) on equal weights:
@@ -331,10 +334,8 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
                 if (ref < 0) {   // merged component: draw (.cu:640-690) and map to world (.cu:1222-1286)
                     const uint32_t key_i = (uint32_t)(-1 - ref);
                     uint32_t w0[4], w1[4];
-                    philox((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 0), prm.key0,
-                           prm.key1, w0);
-                    philox((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 1), prm.key0,
-                           prm.key1, w1);
+                    philox_rk((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 0), prm.rk, w0);
+                    philox_rk((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 1), prm.rk, w1);
                     T z[6];
                     Pair<T>::two(w0[0], w0[1], z[0], z[1]);
                     Pair<T>::two(w0[2], w0[3], z[2], z[3]);
@@ -353,8 +354,7 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
                 }
                 if (has_pred) {   // predict_features with feature noise
                     uint32_t w[4];
-                    philox((uint32_t)s, (uint32_t)j, (uint32_t)p, ctr_word3(pred_frame, ST_FEAT, 0), prm.key0,
-                           prm.key1, w);
+                    philox_rk((uint32_t)s, (uint32_t)j, (uint32_t)p, ctr_word3(pred_frame, ST_FEAT, 0), prm.rk, w);
                     T z[4];
                     Pair<T>::two(w[0], w[1], z[0], z[1]);
                     Pair<T>::two(w[2], w[3], z[2], z[3]);
