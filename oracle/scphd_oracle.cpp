@@ -131,6 +131,32 @@ bool is_pos_def6(const double* cov) {                                 // device_
     return true;
 }
 
+// PD test of an update's posterior covariance.  The reference's isPosDef (a Cholesky
+// without NaN) is decided by the sign of a rounding error when the posterior is exactly
+// singular, as it is after refitting a cloud with fewer in-view samples than dimensions;
+// here (and on the device) such a matrix is classed not PD: every pivot must exceed
+// 1e-10 of its diagonal entry.  Elsewhere the two tests agree.
+bool is_pos_def6_strict(const double* cov) {
+    double L[36];
+    for (int i = 0; i < 36; ++i) L[i] = 0.0;
+    for (int i = 0; i < 6; ++i) {
+        for (int j = 0; j <= i; ++j) {
+            double tmp = cov[i + j * 6];
+            if (i == j) {
+                for (int k = 0; k < j; ++k) tmp -= L[j + k * 6] * L[j + k * 6];
+                if (!(tmp > 1e-10 * cov[i + i * 6])) return false;
+                L[i + j * 6] = std::sqrt(tmp);
+            } else {
+                for (int k = 0; k < j; ++k) tmp -= L[i + k * 6] * L[j + k * 6];
+                L[i + j * 6] = tmp / L[j + j * 6];
+            }
+        }
+    }
+    for (int i = 0; i < 36; ++i)
+        if (std::isnan(L[i])) return false;
+    return true;
+}
+
 void triangular_inverse(const double* L, double* Li, int n) {         // device_math.cu:153-175
     for (int col = 0; col < n; ++col)
         for (int i = 0; i < n; ++i) {
@@ -466,7 +492,7 @@ struct Oracle {
                 for (int a = 0; a < K; ++a) s += Kg[r + a * 6] * Rv[a] * Kg[c + a * 6];
                 out.cov[r + c * 6] = s;
             }
-        if (!is_pos_def6(out.cov)) out.w = safe_log(0);   // kernels.cu:597-598
+        if (!is_pos_def6_strict(out.cov)) out.w = safe_log(0);   // kernels.cu:597-598
     }
 
     static double lse(double a, double b) {   // log_sum_exp functor, .cu:506-517
@@ -584,7 +610,7 @@ struct Oracle {
             for (size_t i = 0; i < comps.size(); ++i) {
                 int m = i < (size_t)G * M ? (int)(i / (size_t)(G > 0 ? G : 1)) : (int)(i - (size_t)G * M);
                 comps[i].w = std::exp(comps[i].w - ell[(size_t)p * M + m]);
-                flags[i] = (comps[i].w < cfg.min_weight) || !is_pos_def6(comps[i].cov);
+                flags[i] = (comps[i].w < cfg.min_weight) || !is_pos_def6_strict(comps[i].cov);
                 survivors[p] += !flags[i];
             }
             // parent log-likelihood, .cu:1813-1849: sum_m ell + sum_j w_j (predicted)

@@ -261,6 +261,36 @@ __device__ inline bool chol6(const T* A, T* L) {
     return ok;
 }
 
+// PD test of an update's posterior covariance: a Cholesky whose every pivot exceeds
+// 1e-10 of its diagonal entry.  Unlike the reference's isPosDef (no NaN in the factor),
+// an exactly singular posterior -- after a refit from fewer in-view samples than
+// dimensions -- is classed not PD instead of by the sign of a rounding error.
+template <typename T>
+__device__ inline bool posterior_pd(const T* A) {
+    T L[21];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+#pragma unroll
+        for (int j = 0; j <= i; ++j) {
+            T tmp = A[tri(i, j)];
+            if (i == j) {
+#pragma unroll
+                for (int k = 0; k < j; ++k) tmp -= L[tri(j, k)] * L[tri(j, k)];
+                if (!(tmp > T(1e-10) * A[tri(i, i)])) return false;
+                L[tri(i, i)] = tsqrt(tmp);
+            } else {
+#pragma unroll
+                for (int k = 0; k < j; ++k) tmp -= L[tri(i, k)] * L[tri(j, k)];
+                L[tri(i, j)] = tmp / L[tri(j, j)];
+            }
+        }
+    }
+    bool ok = true;
+#pragma unroll
+    for (int i = 0; i < 21; ++i) ok = ok && !isnan(L[i]);
+    return ok;
+}
+
 // squared Mahalanobis distance of computeMahalDist<6,36> (src/device_math.cu:374-454):
 // Cholesky of (Sa + Sb), triangular inverse (:153-175), sum_i (sum_{j<=i} dj Linv_ij)^2
 template <typename T>
@@ -406,8 +436,7 @@ __device__ inline void kalman_prep(T w, T pdbar, const T* P, const Model& m, T* 
         Pn[e] = sv;
         dst[kPrepCov + e] = sv;
     }
-    T L[21];
-    const bool pdok = chol6(Pn, L);
+    const bool pdok = posterior_pd(Pn);
     dst[0] = cst;
     dst[1] = pdok ? T(1) : T(0);
 #pragma unroll
