@@ -233,7 +233,7 @@ public:
         a.cap = probe.used;
         carve(a);
         CUDA_TRY(cudaMemsetAsync(p, 0, probe.used, stream));
-        merge_smem = merge_smem_bytes<T>(prm.Scap, prm.Gcap, 4);
+        merge_smem = merge_smem_bytes<T>(prm.Scap, prm.Gcap, kMergeThreads / 32);
         fit_smem = cloud_fit_smem_bytes<T>(prm.P);
         if (fit_smem > 220 * 1024)   // with the kernel's static shared memory, within 227 KB per block
             return fail(SCPHD_ERR_CAPACITY, "particles_per_feature needs " + std::to_string(fit_smem) +
@@ -308,7 +308,7 @@ public:
             stage_end(h);
         }
         h = stage_begin(3);
-        k_merge<T, K><<<N, 128, merge_smem, stream>>>(prm, b, cur, M, fixed);
+        k_merge<T, K><<<N, kMergeThreads, merge_smem, stream>>>(prm, b, cur, M, fixed);
         LAUNCHED();
         stage_end(h);
         h = stage_begin(4);
@@ -1126,7 +1126,7 @@ template <typename T> struct Batch final : scphd_batch {
                     for (int k = 0; k < mb; ++k) ml.back().push_back(make_int4(i, q, k, 0));
                 stage_off[first + i] = stage_total;
                 stage_total += 3 * (size_t)pr.Mcap;
-                merge_smem = std::max(merge_smem, merge_smem_bytes<T>(pr.Scap, pr.Gcap, 4));
+                merge_smem = std::max(merge_smem, merge_smem_bytes<T>(pr.Scap, pr.Gcap, kMergeThreads / 32));
                 fit_smem = std::max(fit_smem, cloud_fit_smem_bytes<T>(pr.P));
                 lik_smem = std::max(lik_smem, likelihood_smem_bytes<T>(pr.Gcap, lik_block));
             }
@@ -1194,7 +1194,7 @@ template <typename T> struct Batch final : scphd_batch {
             LAUNCHED();
         }
         for (const Group& g : groups) {
-            k_merge_batch<T, KK><<<g.n_parent, 128, merge_smem, stream>>>(*g.tab, d_fa + g.first, g.map_parent);
+            k_merge_batch<T, KK><<<g.n_parent, kMergeThreads, merge_smem, stream>>>(*g.tab, d_fa + g.first, g.map_parent);
             LAUNCHED();
         }
         for (const Group& g : groups) {

@@ -930,7 +930,8 @@ template <typename T> struct MergeScratch {
     int nchunk;
 };
 
-constexpr int kSmallComp = 8;   // components up to this size are merged by one thread
+constexpr int kSmallComp = 8;       // components up to this size are merged by one thread
+constexpr int kMergeThreads = 256;   // threads of a parent's merge block (8 warps)
 
 __host__ __device__ inline int next_pow2(int x) {
     int p = 1;
@@ -1407,7 +1408,7 @@ __device__ __forceinline__ void merge_body(const Params& prm, const Bufs<T>& b, 
         }
     }
     // parent log-likelihood: sum_m ell + sum_j w_j (.cu:1813-1849), FP64
-    __shared__ double s_red[4];
+    __shared__ double s_red[32];
     double part = 0;
     for (int mm = tid; mm < M; mm += blockDim.x) part += (double)b.ell[(size_t)p * prm.Mcap + mm];
     for (int j = tid; j < G; j += blockDim.x) part += (double)b.fit[((size_t)p * prm.Gcap + j) * kRow];
@@ -1415,7 +1416,11 @@ __device__ __forceinline__ void merge_body(const Params& prm, const Bufs<T>& b, 
     for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
     if ((tid & 31) == 0) s_red[tid >> 5] = part;
     __syncthreads();
-    if (tid == 0) b.loglik[p] = s_red[0] + s_red[1] + s_red[2] + s_red[3];
+    if (tid == 0) {
+        double t = 0;
+        for (int w2 = 0; w2 < (int)(blockDim.x >> 5); ++w2) t += s_red[w2];
+        b.loglik[p] = t;
+    }
     sort_survivors(s_w, s_key, s_r, n_pad);
     KalmanSource<T, K> src;
     src.fit = b.fit + (size_t)p * prm.Gcap * kRow;
@@ -1536,13 +1541,13 @@ __device__ __forceinline__ void merge_body(const Params& prm, const Bufs<T>& b, 
 }
 
 template <typename T, int K>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 3) k_merge(__grid_constant__ const Params prm, __grid_constant__ const Bufs<T> b,
+__global__ void __launch_bounds__(kMergeThreads, sizeof(T) == 4 ? 3 : 2) k_merge(__grid_constant__ const Params prm, __grid_constant__ const Bufs<T> b,
                                                int cur, int M, int fixed) {
     merge_body<T, K>(prm, b, cur, M, fixed, blockIdx.x);
 }
 
 template <typename T, int K>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 3)
+__global__ void __launch_bounds__(kMergeThreads, sizeof(T) == 4 ? 3 : 2)
     k_merge_batch(const __grid_constant__ SlotTable<T> tab, const FrameArgs* fas, const int2* map) {
     const int2 fp = map[blockIdx.x];
     const FrameArgs fa = fas[fp.x];
