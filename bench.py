@@ -242,6 +242,7 @@ def run_b200(args):
     for _ in range(args.prefill + W):
         dstep()
     filt.synchronize()
+    shapes = filt.launch_shapes()   # tuned on the untimed frames
     stream = torch.cuda.ExternalStream(filt.stream_handle)
     c0 = filt.counters()
     l0 = pkg.kernel_launches()
@@ -357,7 +358,7 @@ def run_b200(args):
                    "mean_gaussians_per_parent": fitted / max(1, K) / cfg.n_parents,
                    "mean_measurements": units / max(1, fitted / K * 1.0) / K if fitted else None,
                    "l2": "no flush: the resident map/cloud state is larger than L2",
-                   "parallelism": f"replicas{world}"},
+                   "parallelism": f"replicas{world}", "launch_shapes": shapes},
         "frame_ms": {"p50": float(np.percentile(frame_ms, 50)), "p99": float(np.percentile(frame_ms, 99)),
                      "max": float(max(frame_ms))},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d // K, "d2h_bytes_per_step": d2h // K},

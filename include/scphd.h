@@ -172,6 +172,16 @@ scphd_status scphd_set_state(scphd_filter* f, const double* states, const double
  * one parent (before the max_survivors cut); [14..15] reserved. */
 scphd_status scphd_get_counters(scphd_filter* f, int64_t counters[16]);
 
+/* Launch shapes tuned on the filter's first updates that have measurements: threads
+ * per merge block (256 or 128) and the likelihood's blocks (1: one block over all of a
+ * parent's measurements, 0: 128-thread blocks).  Each of the four combinations runs
+ * twice, timed with events (those updates wait for the previous one), and the fastest is
+ * kept.  Results do not depend on the shape.  enable = 0 stops tuning and keeps
+ * (256, 1); *tuned = 1 once a choice is made.  No reference counterpart. */
+scphd_status scphd_set_autotune(scphd_filter* f, int32_t enable);
+scphd_status scphd_get_launch_shapes(scphd_filter* f, int32_t* merge_threads, int32_t* likelihood_full,
+                                     int32_t* tuned);
+
 /* The configuration the filter was created with. */
 scphd_status scphd_get_config(scphd_filter* f, scphd_config* out);
 

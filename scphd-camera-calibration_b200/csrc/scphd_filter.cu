@@ -92,6 +92,39 @@ struct scphd_filter {
     int last_M = 0;
     cudaStream_t own_stream = nullptr;   // the handle's stream while the filter is in a batch
     void* batch = nullptr;               // the batch this filter belongs to, if any
+    // Launch shapes that leave every result unchanged, tuned on the first updates that
+    // have measurements: threads per merge block, and whether the likelihood runs one
+    // block over all of a parent's measurements or 128-thread blocks.  Each shape runs
+    // twice, the likelihood and merge are timed with events, the fastest is kept.
+    struct Shape { int merge_threads; int lik_full; };
+    static constexpr int kShapes = 4;
+    const Shape shapes[kShapes] = {{kMergeThreads, 1}, {128, 1}, {kMergeThreads, 0}, {128, 0}};
+    bool tuning = true;
+    int tune_trials = 0;
+    int tune_pending = -1;
+    double tune_ms[kShapes] = {0, 0, 0, 0};
+    int chosen = 0;
+    cudaEvent_t tune_ev[2] = {nullptr, nullptr};
+    // the shape for the next update, and whether it is timed
+    int pick_shape(bool can_time, bool& timed) {
+        timed = tuning && can_time;
+        return timed ? tune_trials % kShapes : chosen;
+    }
+    // fold in the last timed update (waits for it)
+    scphd_status tune_collect() {
+        if (tune_pending < 0) return SCPHD_OK;
+        CUDA_TRY(cudaEventSynchronize(tune_ev[1]));
+        float ms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&ms, tune_ev[0], tune_ev[1]));
+        tune_ms[tune_pending] += ms;
+        tune_pending = -1;
+        if (++tune_trials >= 2 * kShapes) {
+            tuning = false;
+            for (int k = 1; k < kShapes; ++k)
+                if (tune_ms[k] < tune_ms[chosen]) chosen = k;
+        }
+        return SCPHD_OK;
+    }
     // opt-in per-stage event timing
     bool profiling = false;
     struct Mark { int stage; cudaEvent_t a, b; };
@@ -135,6 +168,8 @@ struct scphd_filter {
     }
     virtual ~scphd_filter() {
         for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
+        for (cudaEvent_t e : tune_ev)
+            if (e) cudaEventDestroy(e);
     }
     virtual scphd_status init() = 0;
     virtual scphd_status predict(double dt) = 0;
@@ -218,6 +253,8 @@ public:
 
     scphd_status init() override {
         CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreate(&tune_ev[0]));
+        CUDA_TRY(cudaEventCreate(&tune_ev[1]));
         CUDA_TRY(cudaEventCreateWithFlags(&stage_ev, cudaEventDisableTiming));
         CUDA_TRY(cudaMallocHost(&h_stage, sizeof(double) * 3 * prm.Mcap));
         Arena probe;
@@ -299,8 +336,15 @@ public:
         LAUNCHED();
         stage_end(h);
         pending = false;
+        {
+            const scphd_status ts = tune_collect();
+            if (ts != SCPHD_OK) return ts;
+        }
+        bool timed = false;
+        const Shape sh = shapes[pick_shape(M > 0, timed)];
+        if (timed) CUDA_TRY(cudaEventRecord(tune_ev[0], stream));
         if (M > 0) {
-            const int bs = likelihood_block(M);
+            const int bs = sh.lik_full ? likelihood_block(M) : 128;
             dim3 grid(N, (M + bs - 1) / bs);
             h = stage_begin(2);
             k_likelihood<T, K><<<grid, bs, likelihood_smem_bytes<T>(prm.Gcap, bs), stream>>>(prm, b, cur, M);
@@ -308,9 +352,13 @@ public:
             stage_end(h);
         }
         h = stage_begin(3);
-        k_merge<T, K><<<N, kMergeThreads, merge_smem, stream>>>(prm, b, cur, M, fixed);
+        k_merge<T, K><<<N, sh.merge_threads, merge_smem, stream>>>(prm, b, cur, M, fixed);
         LAUNCHED();
         stage_end(h);
+        if (timed) {
+            CUDA_TRY(cudaEventRecord(tune_ev[1], stream));
+            tune_pending = tune_trials % kShapes;
+        }
         h = stage_begin(4);
         k_weights<<<1, 1024, 0, stream>>>(N, b.lw, b.loglik, fixed ? 0 : 1, b.scal, b.counters);
         LAUNCHED();
@@ -794,6 +842,26 @@ scphd_status scphd_get_config(scphd_filter* f, scphd_config* out) {
     return SCPHD_OK;
 }
 
+scphd_status scphd_set_autotune(scphd_filter* f, int32_t enable) {
+    if (!f) return fail(SCPHD_ERR_INVALID, "null handle");
+    if (!enable) {
+        f->tuning = false;
+        f->tune_pending = -1;
+        f->chosen = 0;
+    }
+    return SCPHD_OK;
+}
+
+scphd_status scphd_get_launch_shapes(scphd_filter* f, int32_t* merge_threads, int32_t* likelihood_full,
+                                     int32_t* tuned) {
+    if (!f) return fail(SCPHD_ERR_INVALID, "null handle");
+    const scphd_filter::Shape& sh = f->shapes[f->chosen];
+    if (merge_threads) *merge_threads = sh.merge_threads;
+    if (likelihood_full) *likelihood_full = sh.lik_full;
+    if (tuned) *tuned = f->tuning ? 0 : 1;
+    return SCPHD_OK;
+}
+
 scphd_status scphd_get_counters(scphd_filter* f, int64_t counters[16]) {
     HANDLE(f);
     if (!counters) return fail(SCPHD_ERR_INVALID, "null output");
@@ -1076,10 +1144,20 @@ template <typename T> struct Batch final : scphd_batch {
     size_t fit_smem = 0;
     size_t lik_smem = 0;
     int lik_block = 32;
+    // threads per merge block, tuned on the first 4 steps (256 and 128, twice each,
+    // before a graph is captured); results do not depend on it
+    int merge_threads = kMergeThreads;
+    bool tuning = true;
+    bool capturing = false;
+    int tune_trials = 0, tune_pending = -1;
+    double tune_ms[2] = {0, 0};
+    cudaEvent_t tune_ev[2] = {nullptr, nullptr};
     void* dev_mem = nullptr;
 
     ~Batch() override {
         if (stream) cudaStreamSynchronize(stream);
+        for (cudaEvent_t e : tune_ev)
+            if (e) cudaEventDestroy(e);
         if (exec) cudaGraphExecDestroy(exec);
         if (done) cudaEventDestroy(done);
         if (h_fa) cudaFreeHost(h_fa);
@@ -1102,6 +1180,8 @@ template <typename T> struct Batch final : scphd_batch {
         K = fs[0]->prm.K;
         CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         CUDA_TRY(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreate(&tune_ev[0]));
+        CUDA_TRY(cudaEventCreate(&tune_ev[1]));
         std::vector<std::vector<int2>> mp, mpred;
         std::vector<std::vector<int4>> ml;
         stage_off.resize(F);
@@ -1193,9 +1273,16 @@ template <typename T> struct Batch final : scphd_batch {
             k_likelihood_batch<T, KK><<<g.n_lik, lik_block, lik_smem, stream>>>(*g.tab, d_fa + g.first, g.map_lik);
             LAUNCHED();
         }
+        const bool timed = tuning && !capturing;
+        const int mt = timed ? (tune_trials % 2 ? 128 : kMergeThreads) : merge_threads;
+        if (timed) CUDA_TRY(cudaEventRecord(tune_ev[0], stream));
         for (const Group& g : groups) {
-            k_merge_batch<T, KK><<<g.n_parent, kMergeThreads, merge_smem, stream>>>(*g.tab, d_fa + g.first, g.map_parent);
+            k_merge_batch<T, KK><<<g.n_parent, mt, merge_smem, stream>>>(*g.tab, d_fa + g.first, g.map_parent);
             LAUNCHED();
+        }
+        if (timed) {
+            CUDA_TRY(cudaEventRecord(tune_ev[1], stream));
+            tune_pending = tune_trials % 2;
         }
         for (const Group& g : groups) {
             k_weights_batch<T><<<g.count, 1024, 0, stream>>>(*g.tab, d_fa + g.first);
@@ -1209,6 +1296,20 @@ template <typename T> struct Batch final : scphd_batch {
     }
 
     int launches_per_frame() const { return 6 * (int)groups.size(); }
+
+    scphd_status tune_collect() {
+        if (tune_pending < 0) return SCPHD_OK;
+        CUDA_TRY(cudaEventSynchronize(tune_ev[1]));
+        float ms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&ms, tune_ev[0], tune_ev[1]));
+        tune_ms[tune_pending] += ms;
+        tune_pending = -1;
+        if (++tune_trials >= 4) {
+            tuning = false;
+            merge_threads = tune_ms[1] < tune_ms[0] ? 128 : kMergeThreads;
+        }
+        return SCPHD_OK;
+    }
 
     scphd_status enqueue() {
         CUDA_TRY(cudaMemcpyAsync(d_stage, h_stage, sizeof(double) * stage_total, cudaMemcpyHostToDevice, stream));
@@ -1267,11 +1368,17 @@ template <typename T> struct Batch final : scphd_batch {
                 fa.zd = K == 3 ? ds + 2 * fr.n : nullptr;
             }
         }
-        if (use_graph) {
+        {
+            const scphd_status ts = tune_collect();
+            if (ts != SCPHD_OK) return ts;
+        }
+        if (use_graph && !tuning) {
             if (!captured) {
                 cudaGraph_t g = nullptr;
                 CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+                capturing = true;
                 scphd_status s = enqueue();
+                capturing = false;
                 cudaError_t e = cudaStreamEndCapture(stream, &g);
                 if (s != SCPHD_OK) return s;
                 if (e != cudaSuccess) return fail(SCPHD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));

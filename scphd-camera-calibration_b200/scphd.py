@@ -194,6 +194,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "scphd_server_stats": (i32, [vp, P(i64)]),
         "scphd_server_step_times": (i32, [vp, i64, i32, P(d), P(i32), P(i32)]),
         "scphd_get_config": (i32, [vp, P(ScphdConfig)]),
+        "scphd_set_autotune": (i32, [vp, i32]),
+        "scphd_get_launch_shapes": (i32, [vp, P(i32), P(i32), P(i32)]),
         "scphd_config_from_file": (i32, [ctypes.c_char_p, P(ScphdConfig), P(ScphdRunOptions)]),
         "scphd_read_mat_frames": (i32, [ctypes.c_char_p, ctypes.c_char_p, P(i32), P(i32), P(i32), P(d), i64]),
         "scphd_write_mat": (i32, [vp, ctypes.c_char_p, i32]),
@@ -367,6 +369,15 @@ class SCPHDCameraCalibration:
         _check(self._lib.scphd_step_device(self._h, float(dt), ctypes.c_void_p(u_ptr), ctypes.c_void_p(v_ptr),
                                            ctypes.c_void_p(d_ptr) if d_ptr else None, int(n),
                                            int(bool(fixed_camera))))
+
+    def set_autotune(self, enable: bool) -> None:
+        """Tune the launch shapes on the first updates (default) or keep the default."""
+        _check(self._lib.scphd_set_autotune(self._h, int(bool(enable))))
+
+    def launch_shapes(self) -> dict:
+        mt, lf, tuned = ctypes.c_int32(0), ctypes.c_int32(0), ctypes.c_int32(0)
+        _check(self._lib.scphd_get_launch_shapes(self._h, ctypes.byref(mt), ctypes.byref(lf), ctypes.byref(tuned)))
+        return {"merge_threads": mt.value, "likelihood_full": bool(lf.value), "tuned": bool(tuned.value)}
 
     def writeMat(self, path: str, save_all_maps: bool = False) -> None:
         """The reference's writeMat: particles, weights and the MAP parent's map (and
