@@ -270,7 +270,7 @@ public:
         a.cap = probe.used;
         carve(a);
         CUDA_TRY(cudaMemsetAsync(p, 0, probe.used, stream));
-        merge_smem = merge_smem_bytes<T>(prm.Scap, prm.Gcap, kMergeThreads / 32);
+        merge_smem = merge_smem_bytes<T>(prm.Scap, prm.Gcap, kMergeThreads / 32, true);
         fit_smem = cloud_fit_smem_bytes<T>(prm.P);
         if (fit_smem > 220 * 1024)   // with the kernel's static shared memory, within 227 KB per block
             return fail(SCPHD_ERR_CAPACITY, "particles_per_feature needs " + std::to_string(fit_smem) +
@@ -886,7 +886,7 @@ scphd_status scphd_merge_components(const double* comps, const uint8_t* flags, i
         uint8_t* d_flags = nullptr;
         int* d_n = nullptr;
         int* d_mem = nullptr;
-        size_t smem = merge_smem_bytes<T>(n + 1, 0, 4);
+        size_t smem = merge_smem_bytes<T>(n + 1, 0, 4, false);
         T* d_sparse = nullptr;
         scphd_status st = SCPHD_OK;
         std::vector<T> out((size_t)n * kRow);
@@ -1008,7 +1008,7 @@ scphd_status merge_static_impl(unsigned char* base, const double* comps, const u
     CUDA_TRY(cudaMemset(d_mem, 0xff, sizeof(int) * (size_t)n));
     k_rows_from28<T><<<(n * kRow + 255) / 256, 256>>>(d_in, n, d_rows);
     g_launches.fetch_add(1, std::memory_order_relaxed);
-    const size_t smem = merge_smem_bytes<T>(n + 1, 0, 4);
+    const size_t smem = merge_smem_bytes<T>(n + 1, 0, 4, false);
     CUDA_TRY(allow_dynamic_smem((const void*)k_merge_list<T>));
     k_merge_list<T><<<1, 128, smem>>>(d_rows, d_flags, n, (T)min_separation, d_sparse, d_out, d_cnt, d_mem);
     g_launches.fetch_add(1, std::memory_order_relaxed);
@@ -1206,7 +1206,7 @@ template <typename T> struct Batch final : scphd_batch {
                     for (int k = 0; k < mb; ++k) ml.back().push_back(make_int4(i, q, k, 0));
                 stage_off[first + i] = stage_total;
                 stage_total += 3 * (size_t)pr.Mcap;
-                merge_smem = std::max(merge_smem, merge_smem_bytes<T>(pr.Scap, pr.Gcap, kMergeThreads / 32));
+                merge_smem = std::max(merge_smem, merge_smem_bytes<T>(pr.Scap, pr.Gcap, kMergeThreads / 32, true));
                 fit_smem = std::max(fit_smem, cloud_fit_smem_bytes<T>(pr.P));
                 lik_smem = std::max(lik_smem, likelihood_smem_bytes<T>(pr.Gcap, lik_block));
             }

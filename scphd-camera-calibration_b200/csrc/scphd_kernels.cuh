@@ -927,6 +927,7 @@ template <typename T> struct MergeScratch {
     int* fill;            // S
     int* perm;            // cap: survivors grouped by component (first: survivors in u order)
     uint32_t* masks;      // (blockDim/32) x nchunk member masks
+    T* mu;                // S x 6 survivor means, or null (then read from the source each time)
     int nchunk;
 };
 
@@ -945,17 +946,21 @@ __host__ __device__ inline int merge_sort_cap(int S, int G) {
     return a > b ? a : b;
 }
 
-template <typename T> inline size_t merge_smem_bytes(int S, int G, int nwarps) {
+// cache_means: the survivors' means are computed once and kept in shared memory
+// (sources whose mean is arithmetic on several rows); sources that read a mean
+// straight from a row leave it off
+template <typename T> inline size_t merge_smem_bytes(int S, int G, int nwarps, bool cache_means) {
     const size_t cap = merge_sort_cap(S, G), nchunk = (S + 31) / 32;
     const size_t pf = 6 * (size_t)S * sizeof(float), pos = (size_t)(S + G) * 4;   // pos aliases pf
-    return cap * (sizeof(T) + 8) + (pf > pos ? pf : pos) + 3 * (size_t)S * 4 + cap * 4 + (size_t)(S + 1) * 4 +
-           (size_t)nwarps * nchunk * 4 + 2 * (size_t)S + 64;
+    return (cache_means ? 6 * (size_t)S * sizeof(T) : 0) + cap * (sizeof(T) + 8) + (pf > pos ? pf : pos) +
+           3 * (size_t)S * 4 + cap * 4 + (size_t)(S + 1) * 4 + (size_t)nwarps * nchunk * 4 + 2 * (size_t)S + 64;
 }
 template <typename T>
-__device__ inline void carve_merge_smem(unsigned char* smem, int S, int G, T*& s_w, uint32_t*& s_key, int*& s_r,
-                                        int*& s_pos, MergeScratch<T>& ms) {
+__device__ inline void carve_merge_smem(unsigned char* smem, int S, int G, bool cache_means, T*& s_w,
+                                        uint32_t*& s_key, int*& s_r, int*& s_pos, MergeScratch<T>& ms) {
     const int cap = merge_sort_cap(S, G);
-    s_w = reinterpret_cast<T*>(smem);
+    ms.mu = cache_means ? reinterpret_cast<T*>(smem) : nullptr;
+    s_w = reinterpret_cast<T*>(smem) + (cache_means ? 6 * S : 0);
     s_key = reinterpret_cast<uint32_t*>(s_w + cap);
     s_r = reinterpret_cast<int*>(s_key + cap);
     ms.pf = reinterpret_cast<float*>(s_r + cap);
@@ -981,12 +986,24 @@ __device__ __forceinline__ bool could_merge_f(const float* a, const float* b, fl
     return ok;
 }
 
+// Mean of sorted survivor i: from the shared cache when there is one (bit-identical
+// to the source's arithmetic: the cache holds its result), else from the source.
+template <typename T, typename Src>
+__device__ __forceinline__ void survivor_mean(const Src& src, const T* mu_cache, const int* s_r, int i, T mu[6]) {
+    if (mu_cache) {
+#pragma unroll
+        for (int a = 0; a < 6; ++a) mu[a] = mu_cache[i * 6 + a];
+    } else {
+        src.mean(s_r[i], mu);
+    }
+}
+
 // Moment-matched merge of the members (ascending survivor indices mem[k] for the set
 // bits k of mbits) into centre c, written to sparse[c]; reference order of the sums
 // (kernels.cu:770-843): weights and weighted means, then covariances about the mean.
 template <typename T, typename Src>
-__device__ void merge_members_thread(const Src& src, const T* s_w, const int* s_r, const int* mem, uint32_t mbits,
-                                     int c, const T* cmu, const T* ccov, T* sparse) {
+__device__ void merge_members_thread(const Src& src, const T* mu_cache, const T* s_w, const int* s_r, const int* mem,
+                                     uint32_t mbits, int c, const T* cmu, const T* ccov, T* sparse) {
     T W = 0, acc[6] = {0, 0, 0, 0, 0, 0};
     for (uint32_t mb = mbits; mb; mb &= mb - 1) {
         int i = mem[__ffs(mb) - 1];
@@ -995,7 +1012,7 @@ __device__ void merge_members_thread(const Src& src, const T* s_w, const int* s_
 #pragma unroll
             for (int a = 0; a < 6; ++a) mu[a] = cmu[a];
         } else {
-            src.mean(s_r[i], mu);
+            survivor_mean(src, mu_cache, s_r, i, mu);
         }
         W += w;
 #pragma unroll
@@ -1015,7 +1032,7 @@ __device__ void merge_members_thread(const Src& src, const T* s_w, const int* s_
 #pragma unroll
             for (int a = 0; a < 6; ++a) mu[a] = cmu[a];
         } else {
-            src.mean(s_r[i], mu);
+            survivor_mean(src, mu_cache, s_r, i, mu);
         }
         const T* sc = src.cov(s_r[i]);
 #pragma unroll
@@ -1128,6 +1145,10 @@ __device__ int merge_components(const Src& src, const T* s_w, const int* s_r, in
     for (int i = tid; i < n; i += blockDim.x) {
         T mu[6];
         src.mean(s_r[i], mu);
+        if (ms.mu) {
+#pragma unroll
+            for (int a = 0; a < 6; ++a) ms.mu[i * 6 + a] = mu[a];
+        }
         const T* cv = src.cov(s_r[i]);
         float* pf = ms.pf + i * 6;
         pf[0] = (float)mu[0]; pf[1] = (float)mu[1]; pf[2] = (float)mu[2];
@@ -1233,7 +1254,7 @@ __device__ int merge_components(const Src& src, const T* s_w, const int* s_r, in
             if (k0 < 0 || k0 >= cnt) break;
             const int cc = mem[k0];
             T cmu[6], ccov[21];
-            src.mean(s_r[cc], cmu);
+            survivor_mean(src, ms.mu, s_r, cc, cmu);
             const T* cp = src.cov(s_r[cc]);
 #pragma unroll
             for (int q = 0; q < 21; ++q) ccov[q] = cp[q];
@@ -1248,14 +1269,14 @@ __device__ int merge_components(const Src& src, const T* s_w, const int* s_r, in
                 if (!could_merge_f(ms.pf + cc * 6, ms.pf + i * 6, fsep, fmargin)) continue;
                 ++evals;
                 T mu[6];
-                src.mean(s_r[i], mu);
+                survivor_mean(src, ms.mu, s_r, i, mu);
                 if (mahal6(cmu, ccov, mu, src.cov(s_r[i])) < min_sep) mbits |= 1u << k;
             }
             if (!mbits) {   // merged weight 0: the reference's loop ends (kernels.cu:783-784)
                 atomicMin(&s_stop, cc);
                 break;
             }
-            merge_members_thread(src, s_w, s_r, mem, mbits, cc, cmu, ccov, sparse);
+            merge_members_thread(src, ms.mu, s_w, s_r, mem, mbits, cc, cmu, ccov, sparse);
             ms.is_center[cc] = 1;
             if (member_out)
                 for (uint32_t mb = mbits; mb; mb &= mb - 1) member_out[s_r[mem[__ffs(mb) - 1]]] = cc;
@@ -1287,7 +1308,7 @@ __device__ int merge_components(const Src& src, const T* s_w, const int* s_r, in
             next = k0 + 1;
             const int cc = mem[k0];
             T cmu[6], ccov[21];
-            src.mean(s_r[cc], cmu);
+            survivor_mean(src, ms.mu, s_r, cc, cmu);
             const T* cp = src.cov(s_r[cc]);
 #pragma unroll
             for (int qq = 0; qq < 21; ++qq) ccov[qq] = cp[qq];
@@ -1300,7 +1321,7 @@ __device__ int merge_components(const Src& src, const T* s_w, const int* s_r, in
                     if (!ms.flag[i] && could_merge_f(ms.pf + cc * 6, ms.pf + i * 6, fsep, fmargin)) {
                         ++evals;
                         T mu[6];
-                        src.mean(s_r[i], mu);
+                        survivor_mean(src, ms.mu, s_r, i, mu);
                         m = mahal6(cmu, ccov, mu, src.cov(s_r[i])) < min_sep;
                     }
                 }
@@ -1319,7 +1340,7 @@ __device__ int merge_components(const Src& src, const T* s_w, const int* s_r, in
                 for (unsigned mk = masks[ch]; mk; mk &= mk - 1) {
                     const int i = mem[ch * 32 + __ffs(mk) - 1];
                     T w = s_w[i], mu[6];
-                    src.mean(s_r[i], mu);
+                    survivor_mean(src, ms.mu, s_r, i, mu);
                     accw += w;
                     T sel = mu[0];
 #pragma unroll
@@ -1348,7 +1369,7 @@ __device__ int merge_components(const Src& src, const T* s_w, const int* s_r, in
                     const int i = mem[ch * 32 + __ffs(mk) - 1];
                     if (lane < 21) {
                         T w = s_w[i], mu[6];
-                        src.mean(s_r[i], mu);
+                        survivor_mean(src, ms.mu, s_r, i, mu);
                         const T* cv = src.cov(s_r[i]);
                         accc += w * (cv[lane] + (mean[ea] - mu[ea]) * (mean[eb] - mu[eb]));
                     }
@@ -1394,7 +1415,7 @@ __device__ __forceinline__ void merge_body(const Params& prm, const Bufs<T>& b, 
     int* s_r;
     int* s_pos;
     MergeScratch<T> ms;
-    carve_merge_smem<T>(smem, prm.Scap, prm.Gcap, s_w, s_key, s_r, s_pos, ms);
+    carve_merge_smem<T>(smem, prm.Scap, prm.Gcap, true, s_w, s_key, s_r, s_pos, ms);
     __shared__ int s_tmp[40];
     for (int i = tid; i < n_pad; i += blockDim.x) {
         if (i < n) {
@@ -1818,7 +1839,7 @@ __global__ void __launch_bounds__(256) k_materialize(Params prm, Bufs<T> b, int 
 
 // ---------------------------------------------------------------- stand-alone merge
 // phdUpdateMergeKernel on an explicit component list (rows of kRow) with prune flags;
-// shared memory as merge_smem_bytes<T>(n_all + 1, 0, 4).
+// shared memory as merge_smem_bytes<T>(n_all + 1, 0, 4, false).
 template <typename T>
 __global__ void __launch_bounds__(128) k_merge_list(const T* rows, const uint8_t* flags_in, int n_all,
                                                     T min_sep, T* sparse, T* out, int* n_out_p, int* member_of) {
@@ -1837,7 +1858,7 @@ __global__ void __launch_bounds__(128) k_merge_list(const T* rows, const uint8_t
     int* s_r;
     int* s_pos;
     MergeScratch<T> ms;
-    carve_merge_smem<T>(smem, n_all + 1, 0, s_w, s_key, s_r, s_pos, ms);
+    carve_merge_smem<T>(smem, n_all + 1, 0, false, s_w, s_key, s_r, s_pos, ms);
     if (threadIdx.x == 0) {
         int k = 0;
         for (int i = 0; i < n_all; ++i)
