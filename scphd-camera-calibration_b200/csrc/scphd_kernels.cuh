@@ -668,12 +668,10 @@ __global__ void __launch_bounds__(1024)
 }
 
 // ---------------------------------------------------------------- (d) merge
-// Component sources for the merge loop: posterior components of one parent
-// (detections and births), or an explicit list.
+// Posterior components of one parent (detections and births) by survivor rank r:
+// the mean from the fitted row, Kalman gain and measurement; the covariance is
+// Gaussian j's posterior (prep rows) or the birth covariance.
 template <typename T, int K> struct KalmanSource {
-    // every component has a PD covariance (posteriors passed the PD test, births are
-    // diagonal), so a centre's distance to itself is exactly 0 < min_separation
-    static constexpr bool kSelfAbsorbs = true;
     const T* fit;   // parent's fitted rows
     const T* prep;  // parent's prep rows
     const T* z;     // measurements
@@ -702,23 +700,40 @@ template <typename T, int K> struct KalmanSource {
             for (int a = 0; a < K; ++a) mu[a] = z[mm * 3 + a];
         }
     }
-    __device__ const T* cov(int r) const {
-        if (r < G * M) {
-            int j = r % G;
-            return prep + (size_t)j * kPrep + kPrepCov;
-        }
-        return bcov;
-    }
 };
 
-template <typename T> struct ListSource {
+// Survivor views of the greedy merge: index i is a survivor's position in the sorted
+// order.  ListView reads a caller's rows in place; KalmanView reads the survivors'
+// means and covariance-row indices staged in shared memory by the merge kernel
+// (cj[i] = the posterior's Gaussian, -1 = a birth) and the covariances from the
+// parent's prep rows.
+template <typename T> struct ListView {
     static constexpr bool kSelfAbsorbs = false;   // caller's rows: the self-distance is evaluated
-    const T* rows;   // n rows of kRow
-    __device__ void mean(int r, T mu[6]) const {
+    const T* rows;
+    const int* s_r;
+    __device__ void mean(int i, T mu[6]) const {
+        const T* r = rows + (size_t)s_r[i] * kRow + 1;
 #pragma unroll
-        for (int a = 0; a < 6; ++a) mu[a] = rows[(size_t)r * kRow + 1 + a];
+        for (int a = 0; a < 6; ++a) mu[a] = r[a];
     }
-    __device__ const T* cov(int r) const { return rows + (size_t)r * kRow + 7; }
+    __device__ const T* cov(int i) const { return rows + (size_t)s_r[i] * kRow + 7; }
+};
+template <typename T> struct KalmanView {
+    // every component has a PD covariance (posteriors passed the PD test, births are
+    // diagonal), so a centre's distance to itself is exactly 0 < min_separation
+    static constexpr bool kSelfAbsorbs = true;
+    const T* mu;      // S x 6
+    const int* cj;    // S
+    const T* covs;    // Gaussian j's covariance at covs + j * kPrep
+    const T* bcov;    // birth covariance (21, shared memory)
+    __device__ void mean(int i, T m[6]) const {
+#pragma unroll
+        for (int a = 0; a < 6; ++a) m[a] = mu[i * 6 + a];
+    }
+    __device__ const T* cov(int i) const {
+        const int j = cj[i];
+        return j >= 0 ? covs + (size_t)j * kPrep : bcov;
+    }
 };
 
 template <typename T> __device__ __forceinline__ bool merge_before(T wa, uint32_t ka, T wb, uint32_t kb) {
@@ -927,7 +942,6 @@ template <typename T> struct MergeScratch {
     int* fill;            // S
     int* perm;            // cap: survivors grouped by component (first: survivors in u order)
     uint32_t* masks;      // (blockDim/32) x nchunk member masks
-    T* mu;                // S x 6 survivor means, or null (then read from the source each time)
     int nchunk;
 };
 
@@ -946,21 +960,24 @@ __host__ __device__ inline int merge_sort_cap(int S, int G) {
     return a > b ? a : b;
 }
 
-// cache_means: the survivors' means are computed once and kept in shared memory
-// (sources whose mean is arithmetic on several rows); sources that read a mean
-// straight from a row leave it off
-template <typename T> inline size_t merge_smem_bytes(int S, int G, int nwarps, bool cache_means) {
+// Survivor staging of the filter's merge (KalmanView) in front of the scratch: means
+// (S x 6), the birth covariance (21) and covariance-row indices (S).  A caller's rows
+// (ListView) are read in place and stage nothing.  (Staging the G posterior
+// covariances as well was measured slower: the copy costs more than the reads save.)
+template <typename T> __host__ __device__ inline size_t merge_stage_bytes(int S, bool stage) {
+    return stage ? (((6 * (size_t)S + 21) * sizeof(T) + 4 * (size_t)S + 15) & ~(size_t)15) : 0;
+}
+template <typename T> inline size_t merge_smem_bytes(int S, int G, int nwarps, bool stage) {
     const size_t cap = merge_sort_cap(S, G), nchunk = (S + 31) / 32;
     const size_t pf = 6 * (size_t)S * sizeof(float), pos = (size_t)(S + G) * 4;   // pos aliases pf
-    return (cache_means ? 6 * (size_t)S * sizeof(T) : 0) + cap * (sizeof(T) + 8) + (pf > pos ? pf : pos) +
-           3 * (size_t)S * 4 + cap * 4 + (size_t)(S + 1) * 4 + (size_t)nwarps * nchunk * 4 + 2 * (size_t)S + 64;
+    return merge_stage_bytes<T>(S, stage) + cap * (sizeof(T) + 8) + (pf > pos ? pf : pos) + 3 * (size_t)S * 4 +
+           cap * 4 + (size_t)(S + 1) * 4 + (size_t)nwarps * nchunk * 4 + 2 * (size_t)S + 64;
 }
 template <typename T>
-__device__ inline void carve_merge_smem(unsigned char* smem, int S, int G, bool cache_means, T*& s_w,
-                                        uint32_t*& s_key, int*& s_r, int*& s_pos, MergeScratch<T>& ms) {
+__device__ inline void carve_merge_smem(unsigned char* smem, int S, int G, bool stage, T*& s_w, uint32_t*& s_key,
+                                        int*& s_r, int*& s_pos, MergeScratch<T>& ms) {
     const int cap = merge_sort_cap(S, G);
-    ms.mu = cache_means ? reinterpret_cast<T*>(smem) : nullptr;
-    s_w = reinterpret_cast<T*>(smem) + (cache_means ? 6 * S : 0);
+    s_w = reinterpret_cast<T*>(smem + merge_stage_bytes<T>(S, stage));
     s_key = reinterpret_cast<uint32_t*>(s_w + cap);
     s_r = reinterpret_cast<int*>(s_key + cap);
     ms.pf = reinterpret_cast<float*>(s_r + cap);
@@ -986,24 +1003,12 @@ __device__ __forceinline__ bool could_merge_f(const float* a, const float* b, fl
     return ok;
 }
 
-// Mean of sorted survivor i: from the shared cache when there is one (bit-identical
-// to the source's arithmetic: the cache holds its result), else from the source.
-template <typename T, typename Src>
-__device__ __forceinline__ void survivor_mean(const Src& src, const T* mu_cache, const int* s_r, int i, T mu[6]) {
-    if (mu_cache) {
-#pragma unroll
-        for (int a = 0; a < 6; ++a) mu[a] = mu_cache[i * 6 + a];
-    } else {
-        src.mean(s_r[i], mu);
-    }
-}
-
 // Moment-matched merge of the members (ascending survivor indices mem[k] for the set
 // bits k of mbits) into centre c, written to sparse[c]; reference order of the sums
 // (kernels.cu:770-843): weights and weighted means, then covariances about the mean.
-template <typename T, typename Src>
-__device__ void merge_members_thread(const Src& src, const T* mu_cache, const T* s_w, const int* s_r, const int* mem,
-                                     uint32_t mbits, int c, const T* cmu, const T* ccov, T* sparse) {
+template <typename T, typename View>
+__device__ void merge_members_thread(const View& v, const T* s_w, const int* mem, uint32_t mbits, int c, const T* cmu,
+                                     const T* ccov, T* sparse) {
     T W = 0, acc[6] = {0, 0, 0, 0, 0, 0};
     for (uint32_t mb = mbits; mb; mb &= mb - 1) {
         int i = mem[__ffs(mb) - 1];
@@ -1012,7 +1017,7 @@ __device__ void merge_members_thread(const Src& src, const T* mu_cache, const T*
 #pragma unroll
             for (int a = 0; a < 6; ++a) mu[a] = cmu[a];
         } else {
-            survivor_mean(src, mu_cache, s_r, i, mu);
+            v.mean(i, mu);
         }
         W += w;
 #pragma unroll
@@ -1032,9 +1037,9 @@ __device__ void merge_members_thread(const Src& src, const T* mu_cache, const T*
 #pragma unroll
             for (int a = 0; a < 6; ++a) mu[a] = cmu[a];
         } else {
-            survivor_mean(src, mu_cache, s_r, i, mu);
+            v.mean(i, mu);
         }
-        const T* sc = src.cov(s_r[i]);
+        const T* sc = v.cov(i);
 #pragma unroll
         for (int a = 0; a < 6; ++a) d[a] = row[1 + a] - mu[a];
 #pragma unroll
@@ -1134,8 +1139,8 @@ __device__ void sort_keys(uint32_t* key, int* val, int n_pad) {
 // of a large one.  Merged rows are written to sparse[centre index]; returns the
 // index of the first centre that absorbed nothing (the reference's loop ends there),
 // or n.  Block-wide call.
-template <typename T, typename Src>
-__device__ int merge_components(const Src& src, const T* s_w, const int* s_r, int n, MergeScratch<T> ms,
+template <typename T, typename View>
+__device__ int merge_components(const View& v, const T* s_w, const int* s_r, int n, MergeScratch<T> ms,
                                 uint32_t* ukey, T min_sep, T* sparse, int* member_out,
                                 unsigned long long* counters) {
     __shared__ int s_ncomp, s_take, s_nlarge, s_take_large, s_stop, s_evals;
@@ -1144,12 +1149,8 @@ __device__ int merge_components(const Src& src, const T* s_w, const int* s_r, in
     const float fsep = (float)min_sep, fmargin = 1.01f;
     for (int i = tid; i < n; i += blockDim.x) {
         T mu[6];
-        src.mean(s_r[i], mu);
-        if (ms.mu) {
-#pragma unroll
-            for (int a = 0; a < 6; ++a) ms.mu[i * 6 + a] = mu[a];
-        }
-        const T* cv = src.cov(s_r[i]);
+        v.mean(i, mu);
+        const T* cv = v.cov(i);
         float* pf = ms.pf + i * 6;
         pf[0] = (float)mu[0]; pf[1] = (float)mu[1]; pf[2] = (float)mu[2];
         pf[3] = (float)cv[0]; pf[4] = (float)cv[2]; pf[5] = (float)cv[5];
@@ -1254,29 +1255,29 @@ __device__ int merge_components(const Src& src, const T* s_w, const int* s_r, in
             if (k0 < 0 || k0 >= cnt) break;
             const int cc = mem[k0];
             T cmu[6], ccov[21];
-            survivor_mean(src, ms.mu, s_r, cc, cmu);
-            const T* cp = src.cov(s_r[cc]);
+            v.mean(cc, cmu);
+            const T* cp = v.cov(cc);
 #pragma unroll
             for (int q = 0; q < 21; ++q) ccov[q] = cp[q];
             uint32_t mbits = 0;
             for (int k = k0; k < cnt; ++k) {
                 if ((done >> k) & 1u) continue;
                 const int i = mem[k];
-                if (Src::kSelfAbsorbs && k == k0) {   // distance to itself: 0
+                if (View::kSelfAbsorbs && k == k0) {   // distance to itself: 0
                     mbits |= 1u << k;
                     continue;
                 }
                 if (!could_merge_f(ms.pf + cc * 6, ms.pf + i * 6, fsep, fmargin)) continue;
                 ++evals;
                 T mu[6];
-                survivor_mean(src, ms.mu, s_r, i, mu);
-                if (mahal6(cmu, ccov, mu, src.cov(s_r[i])) < min_sep) mbits |= 1u << k;
+                v.mean(i, mu);
+                if (mahal6(cmu, ccov, mu, v.cov(i)) < min_sep) mbits |= 1u << k;
             }
             if (!mbits) {   // merged weight 0: the reference's loop ends (kernels.cu:783-784)
                 atomicMin(&s_stop, cc);
                 break;
             }
-            merge_members_thread(src, ms.mu, s_w, s_r, mem, mbits, cc, cmu, ccov, sparse);
+            merge_members_thread(v, s_w, mem, mbits, cc, cmu, ccov, sparse);
             ms.is_center[cc] = 1;
             if (member_out)
                 for (uint32_t mb = mbits; mb; mb &= mb - 1) member_out[s_r[mem[__ffs(mb) - 1]]] = cc;
@@ -1308,8 +1309,8 @@ __device__ int merge_components(const Src& src, const T* s_w, const int* s_r, in
             next = k0 + 1;
             const int cc = mem[k0];
             T cmu[6], ccov[21];
-            survivor_mean(src, ms.mu, s_r, cc, cmu);
-            const T* cp = src.cov(s_r[cc]);
+            v.mean(cc, cmu);
+            const T* cp = v.cov(cc);
 #pragma unroll
             for (int qq = 0; qq < 21; ++qq) ccov[qq] = cp[qq];
             bool any = false;
@@ -1321,8 +1322,8 @@ __device__ int merge_components(const Src& src, const T* s_w, const int* s_r, in
                     if (!ms.flag[i] && could_merge_f(ms.pf + cc * 6, ms.pf + i * 6, fsep, fmargin)) {
                         ++evals;
                         T mu[6];
-                        survivor_mean(src, ms.mu, s_r, i, mu);
-                        m = mahal6(cmu, ccov, mu, src.cov(s_r[i])) < min_sep;
+                        v.mean(i, mu);
+                        m = mahal6(cmu, ccov, mu, v.cov(i)) < min_sep;
                     }
                 }
                 const unsigned bal = __ballot_sync(0xffffffffu, m);
@@ -1340,7 +1341,7 @@ __device__ int merge_components(const Src& src, const T* s_w, const int* s_r, in
                 for (unsigned mk = masks[ch]; mk; mk &= mk - 1) {
                     const int i = mem[ch * 32 + __ffs(mk) - 1];
                     T w = s_w[i], mu[6];
-                    survivor_mean(src, ms.mu, s_r, i, mu);
+                    v.mean(i, mu);
                     accw += w;
                     T sel = mu[0];
 #pragma unroll
@@ -1369,8 +1370,8 @@ __device__ int merge_components(const Src& src, const T* s_w, const int* s_r, in
                     const int i = mem[ch * 32 + __ffs(mk) - 1];
                     if (lane < 21) {
                         T w = s_w[i], mu[6];
-                        survivor_mean(src, ms.mu, s_r, i, mu);
-                        const T* cv = src.cov(s_r[i]);
+                        v.mean(i, mu);
+                        const T* cv = v.cov(i);
                         accc += w * (cv[lane] + (mean[ea] - mu[ea]) * (mean[eb] - mu[eb]));
                     }
                 }
@@ -1458,8 +1459,29 @@ __device__ __forceinline__ void merge_body(const Params& prm, const Bufs<T>& b, 
     src.bcov[tri(3, 3)] = (T)prm.var_vu0;
     src.bcov[tri(4, 4)] = (T)prm.var_vv0;
     src.bcov[tri(5, 5)] = (T)prm.var_vd0;
+    // survivors' means and covariance rows staged once (each is read several times)
+    KalmanView<T> view;
+    {
+        T* st_mu = reinterpret_cast<T*>(smem);
+        T* st_bcov = st_mu + 6 * prm.Scap;
+        int* st_cj = reinterpret_cast<int*>(st_bcov + 21);
+        for (int i = tid; i < n; i += blockDim.x) {
+            const int r = s_r[i];
+            T mu[6];
+            src.mean(r, mu);
+#pragma unroll
+            for (int a = 0; a < 6; ++a) st_mu[i * 6 + a] = mu[a];
+            st_cj[i] = r < G * M ? r % G : -1;
+        }
+        if (tid < 21) st_bcov[tid] = src.bcov[tid];
+        view.covs = src.prep + kPrepCov;
+        view.mu = st_mu;
+        view.cj = st_cj;
+        view.bcov = st_bcov;
+        __syncthreads();
+    }
     T* sparse = b.mtmp + (size_t)p * prm.Scap * kRow;
-    const int stop = merge_components<T>(src, s_w, s_r, n, ms, s_key, (T)prm.min_sep, sparse, nullptr, b.counters);
+    const int stop = merge_components<T>(view, s_w, s_r, n, ms, s_key, (T)prm.min_sep, sparse, nullptr, b.counters);
     // merged list in centre order (centres after a stop are dropped, as the reference's loop ends there)
     for (int i = tid; i < n; i += blockDim.x) s_pos[i] = (i < stop && ms.is_center[i]) ? 1 : 0;
     __syncthreads();
@@ -1872,8 +1894,8 @@ __global__ void __launch_bounds__(128) k_merge_list(const T* rows, const uint8_t
     }
     __syncthreads();
     sort_survivors(s_w, s_key, s_r, n_pad);
-    ListSource<T> src{rows};
-    const int stop = merge_components<T>(src, s_w, s_r, n, ms, s_key, min_sep, sparse, member_of, nullptr);
+    ListView<T> view{rows, s_r};
+    const int stop = merge_components<T>(view, s_w, s_r, n, ms, s_key, min_sep, sparse, member_of, nullptr);
     for (int i = threadIdx.x; i < n; i += blockDim.x) s_pos[i] = (i < stop && ms.is_center[i]) ? 1 : 0;
     __syncthreads();
     const int n_out = block_exclusive_scan(s_pos, n, s_tmp);
