@@ -139,24 +139,27 @@ __global__ void k_predict_parents(__grid_constant__ const Params prm, double* ex
 }
 
 // ---------------------------------------------------------------- (b) cloud -> fit
-// One CTA per parent, one warp per daughter Gaussian; lane l owns samples
-// l, l+32, ... .  Covers: predict_features + ps (.cu:154-178, 1144-1150),
+// One CTA per parent; each warp takes the parent's daughter Gaussians in pairs, lanes
+// 0-15 owning samples l, l+16, ... of the first and lanes 16-31 those of the second.
+// Covers: predict_features + ps (.cu:154-178, 1144-1150),
 // worldToDisparityKernel + computePdKernel (kernels.cu:6-47, 82-99), weight by pD
 // (.cu:1602-1609), normalizeWeightsKernel + fitGaussiansKernel (kernels.cu:996-1018,
 // 102-438) and the non-detection copy (.cu:1290-1420).
 //
 // Each sample is generated (merged component: drawn from its stored Gaussian with
 // the counter-based stream; non-detection cloud: loaded), predicted, transformed,
-// and staged in the warp's shared-memory rows as d = y - shift (shift: the warp's
-// first sample, if finite) with its weight w'_s = omega_s pD_s.  The 29 moments are
-// then summed lane by lane (lane q owns moment q: S0 = sum w', S2 = sum w'^2,
-// S1 = sum w' d, SS = sum w' d d'), so no per-lane accumulators live through the
-// sample loop.  With the reference's normalised weights w'_s / S0, mean = shift +
-// S1/S0 and the weighted covariance is (SS/S0 - d d') (1 + S2/S0^2), d = S1/S0 (the
-// (W^2 + SS)/W normaliser of kernels.cu:196 with W = 1).  Zero-weight samples do not
-// enter the sums (their staged d is cleared).  When S0 = 0 the reference weights
-// every sample by 1; that fit matters only when the mean pD is positive (some sample
-// weight omega = 0), and is computed from the staged rows.  A non-detection cloud is
+// and staged in the warp's shared-memory rows with its weight w'_s = omega_s pD_s as
+// r d, r and w', where d = y - shift (shift: the Gaussian's first sample, if finite)
+// and r = sqrt(w').  The 29 moments are then summed lane by lane, one product of two
+// rows each (lane q owns moment q: S0 = sum r r, S2 = sum w' w', S1 = sum r (r d),
+// SS = sum (r d)(r d)'), so no per-lane accumulators live through the sample loop.
+// With the reference's normalised weights w'_s / S0, mean = shift + S1/S0 and the
+// weighted covariance is (SS/S0 - d d') (1 + S2/S0^2), d = S1/S0 (the (W^2 + SS)/W
+// normaliser of kernels.cu:196 with W = 1).  Zero-weight samples do not enter the sums
+// (they stage zeros).  When S0 = 0 the reference weights every sample by 1; that fit
+// matters only when the mean pD is positive (some sample weight omega = 0, possible
+// only with pD = 1), and is computed from the raw samples, drawn a second time for
+// it.  A non-detection cloud is
 // kept only if W (1 - pD_mean) >= min_weight (nd_weight, the merge's test), which needs
 // W >= min_weight: clouds with W >= min_weight are written while streaming (with
 // evict-first stores: they are read again only next frame) and the new map references
@@ -194,52 +197,51 @@ __device__ __forceinline__ void ltz_plus_mean(const double* line, const double z
     ltz_line<double, double2, 2>(line, z, y);
 }
 
-// sum over s < n (n a multiple of 4) of w[s] a[s] b[s], four partial sums, rows read
-// in 16-byte pieces (row starts are 16-byte aligned)
-__device__ __forceinline__ float moment_sweep(const float* w, const float* a, const float* b, int n) {
-    const float4* w4 = reinterpret_cast<const float4*>(w);
+// sum over s < n (n a multiple of 4) of a[s] b[s], four partial sums, rows read in
+// 16-byte pieces (row starts are 16-byte aligned)
+__device__ __forceinline__ float moment_sweep(const float* a, const float* b, int n) {
     const float4* a4 = reinterpret_cast<const float4*>(a);
     const float4* b4 = reinterpret_cast<const float4*>(b);
     float s0 = 0, s1 = 0, s2 = 0, s3 = 0;
     for (int i = 0; i < (n >> 2); ++i) {
-        const float4 x = w4[i], y = a4[i], z = b4[i];
-        s0 += x.x * y.x * z.x;
-        s1 += x.y * y.y * z.y;
-        s2 += x.z * y.z * z.z;
-        s3 += x.w * y.w * z.w;
+        const float4 y = a4[i], z = b4[i];
+        s0 += y.x * z.x;
+        s1 += y.y * z.y;
+        s2 += y.z * z.z;
+        s3 += y.w * z.w;
     }
     return (s0 + s1) + (s2 + s3);
 }
-__device__ __forceinline__ double moment_sweep(const double* w, const double* a, const double* b, int n) {
-    const double2* w2 = reinterpret_cast<const double2*>(w);
+__device__ __forceinline__ double moment_sweep(const double* a, const double* b, int n) {
     const double2* a2 = reinterpret_cast<const double2*>(a);
     const double2* b2 = reinterpret_cast<const double2*>(b);
     double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
     for (int i = 0; i < (n >> 2); ++i) {
-        const double2 x = w2[2 * i], y = a2[2 * i], z = b2[2 * i];
-        const double2 x1 = w2[2 * i + 1], y1 = a2[2 * i + 1], z1 = b2[2 * i + 1];
-        s0 += x.x * y.x * z.x;
-        s1 += x.y * y.y * z.y;
-        s2 += x1.x * y1.x * z1.x;
-        s3 += x1.y * y1.y * z1.y;
+        const double2 y = a2[2 * i], z = b2[2 * i];
+        const double2 y1 = a2[2 * i + 1], z1 = b2[2 * i + 1];
+        s0 += y.x * z.x;
+        s1 += y.y * z.y;
+        s2 += y1.x * z1.x;
+        s3 += y1.y * z1.y;
     }
     return (s0 + s1) + (s2 + s3);
 }
 
 // Staged sample rows: each warp works on Gaussians in pairs and stages, per Gaussian of
-// the pair, 8 rows of P4 = round_up(P, 4) values: the samples' (u, v, d, vu, vv, vd),
-// their weights w', and ones.  The row stride is P4 or the next size whose rows start
-// an odd multiple of 4 banks apart, so that the eight rows a lane-per-moment sweep reads
-// at one sample index (16-byte pieces) fall in distinct banks.
+// the pair, 8 rows of P4 = round_up(P, 4) values: r d for (u, v, d, vu, vv, vd), r and
+// w'.  The row stride is P4 or the next size whose rows start an odd multiple of 4
+// banks apart, so that the eight rows a lane-per-moment sweep reads at one sample
+// index (16-byte pieces) fall in distinct banks; the second Gaussian's rows start 16
+// values further on, so that the two half-warps' stores of one row never share a bank.
 template <typename T> __host__ __device__ inline int stage_stride(int P4) {
     if (sizeof(T) == 4) return (P4 % 8 == 4) ? P4 : P4 + 4;
     return P4 + 2;
 }
 constexpr int kFitWarps = 8;
-constexpr int kStageRows = 8;   // y[6], w', ones
+constexpr int kStageRows = 8;   // r d[6], r, w'
 template <typename T> __host__ __device__ inline size_t cloud_fit_smem_bytes(int P) {
     const int P4 = (P + 3) & ~3;
-    const size_t stage = (size_t)kFitWarps * 2 * kStageRows * stage_stride<T>(P4);   // sample rows
+    const size_t stage = (size_t)kFitWarps * 2 * (kStageRows * stage_stride<T>(P4) + 16);   // sample rows
     const size_t prep = (size_t)kFitWarps * 32 * 42;                                  // per-thread Kalman scratch
     return (stage > prep ? stage : prep) * sizeof(T);
 }
@@ -262,7 +264,8 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
     const int P = prm.P, Ps = prm.Ps;
     const int P4 = (P + 3) & ~3;
     const int sY = stage_stride<T>(P4);
-    T* Ywarp = s_stage + (size_t)warp * 2 * kStageRows * sY;   // per Gaussian of the pair: y[6], w', ones
+    T* Ywarp = s_stage + (size_t)warp * 2 * (kStageRows * sY + 16);   // per Gaussian of the pair: r d[6], r, w'
+    __shared__ T s_shift[kFitWarps * 2 * 6];   // per warp and Gaussian: the moments' shift
     __shared__ Pose<T> pose_upd, pose_src;
     __shared__ int s_rd, s_wr;
     __shared__ __align__(16) T s_L[kFitWarps * 2 * 28];   // per warp and Gaussian: Cholesky factor and mean
@@ -277,19 +280,16 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
         s_rd = 0;
         s_wr = 0;
     }
-    for (int s = lane; s < sY; s += 32) {
-        Ywarp[7 * sY + s] = T(1);
-        Ywarp[(kStageRows + 7) * sY + s] = T(1);
-    }
     __syncthreads();
     const Model& m = prm.model;
     const T invP = T(1) / T(P);
     const T dtT = (T)dt, half_dt2 = T(0.5) * (T)dt * (T)dt;
     T* fitw = s_fit + warp * 32;
-    // moment owned by this lane: rows (ra, rb) of the weighted product w' * Y[ra] * Y[rb]
-    int ra = 7, rb = 7;
-    if (lane == 1) ra = 6;
-    else if (lane >= 2 && lane < 8) ra = lane - 2;
+    // moment owned by this lane: rows (ra, rb) of the product Y[ra] * Y[rb]: lane 0
+    // S0 = sum r r, lane 1 S2 = sum w' w', lanes 2-7 S1 = sum r (r d), lanes 8-28 SS
+    int ra = 6, rb = 6;
+    if (lane == 1) ra = rb = 7;
+    else if (lane >= 2 && lane < 8) rb = lane - 2;
     else if (lane >= 8 && lane < 29) {
         int e = lane - 8, aa = 0;
         while ((aa + 1) * (aa + 2) / 2 <= e) ++aa;
@@ -318,108 +318,120 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
             }
         }
         __syncwarp();
-        const bool wnd0 = Wg[0] >= (T)prm.min_weight, wnd1 = Wg[1] >= (T)prm.min_weight;
-        const int total = nG * P;
-        int n_in0 = 0, n_in1 = 0;
-        bool any0 = false, any1 = false;
-        for (int t = 0; t * 32 < total; ++t) {
-            const int f = lane + 32 * t;
-            const bool valid = f < total;
-            const int g = f >= P ? 1 : 0;
-            const int s = f - g * P;
-            const int ref = g ? refg[1] : refg[0];
-            const int j = j0 + g;
-            T X[6], om = 0, y[6];
-            if (valid) {
-                if (ref < 0) {   // merged component: draw (.cu:640-690) and map to world (.cu:1222-1286)
-                    const uint32_t key_i = (uint32_t)(-1 - ref);
-                    uint32_t w0[4], w1[4];
-                    philox_rk((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 0), prm.rk, w0);
-                    philox_rk((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 1), prm.rk, w1);
-                    T z[6];
-                    Pair<T>::two(w0[0], w0[1], z[0], z[1]);
-                    Pair<T>::two(w0[2], w0[3], z[2], z[3]);
-                    Pair<T>::two(w1[0], w1[1], z[4], z[5]);
-                    T yy[6];
-                    ltz_plus_mean(s_L + (warp * 2 + g) * 28, z, yy);   // y = L z + mean
-                    invert(yy, pose_src, m, X);
-                    om = invP;
-                } else {         // non-detection cloud carried from the previous frame
-                    // the previous frame's clouds are only read in this kernel (writes go to
-                    // the other buffer): read-only loads, free to move ahead of the stores
-                    const T* cl_in = b.cloud[cur] + (size_t)ref * 7 * Ps;
+        // lanes 0-15 sample Gaussian j0, lanes 16-31 Gaussian j0 + 1, 16 samples each per pass
+        const int g = lane >> 4, hl = lane & 15;
+        const bool gvalid = g < nG;
+        const int ref = g ? refg[1] : refg[0];
+        const int j = j0 + g;
+        const bool wnd = (g ? Wg[1] : Wg[0]) >= (T)prm.min_weight;
+        T* Y = Ywarp + (size_t)g * (kStageRows * sY + 16);
+        T* shift_g = s_shift + (warp * 2 + g) * 6;
+        int n_in = 0;
+        bool any = false;
+        // raw = false: stage the moment rows (see above) and write the non-detection
+        // clouds; raw = true (fallback fit only): stage y itself where `stage`, write nothing
+        auto sample_pass = [&](bool raw, bool stage) {
+            n_in = 0;
+            any = false;
+            T shift[6];
+            for (int t = 0; 16 * t < P4; ++t) {
+                const int s = 16 * t + hl;
+                const bool valid = gvalid && s < P;
+                T X[6], om = 0, y[6];
+                if (valid) {
+                    if (ref < 0) {   // merged component: draw (.cu:640-690) and map to world (.cu:1222-1286)
+                        const uint32_t key_i = (uint32_t)(-1 - ref);
+                        uint32_t w0[4], w1[4];
+                        philox_rk((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 0), prm.rk, w0);
+                        philox_rk((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 1), prm.rk, w1);
+                        T z[6];
+                        Pair<T>::two(w0[0], w0[1], z[0], z[1]);
+                        Pair<T>::two(w0[2], w0[3], z[2], z[3]);
+                        Pair<T>::two(w1[0], w1[1], z[4], z[5]);
+                        T yy[6];
+                        ltz_plus_mean(s_L + (warp * 2 + g) * 28, z, yy);   // y = L z + mean
+                        invert(yy, pose_src, m, X);
+                        om = invP;
+                    } else {         // non-detection cloud carried from the previous frame
+                        // the previous frame's clouds are only read in this kernel (writes go to
+                        // the other buffer): read-only loads, free to move ahead of the stores
+                        const T* cl_in = b.cloud[cur] + (size_t)ref * 7 * Ps;
 #pragma unroll
-                    for (int a2 = 0; a2 < 6; ++a2) X[a2] = __ldg(cl_in + a2 * Ps + s);
-                    om = __ldg(cl_in + 6 * Ps + s);
+                        for (int a2 = 0; a2 < 6; ++a2) X[a2] = __ldg(cl_in + a2 * Ps + s);
+                        om = __ldg(cl_in + 6 * Ps + s);
+                    }
+                    if (has_pred) {   // predict_features with feature noise
+                        uint32_t w[4];
+                        philox_rk((uint32_t)s, (uint32_t)j, (uint32_t)p, ctr_word3(pred_frame, ST_FEAT, 0), prm.rk, w);
+                        T z[4];
+                        Pair<T>::two(w[0], w[1], z[0], z[1]);
+                        Pair<T>::two(w[2], w[3], z[2], z[3]);
+#pragma unroll
+                        for (int q = 0; q < 3; ++q) {
+                            T a2 = (T)prm.feat_std[q] * z[q];
+                            X[q] = X[q] + X[q + 3] * dtT + a2 * half_dt2;
+                            X[q + 3] = X[q + 3] + a2 * dtT;
+                        }
+                    }
+                    measure(X, pose_upd, m, y);
+                } else {
+#pragma unroll
+                    for (int a2 = 0; a2 < 6; ++a2) { X[a2] = 0; y[a2] = 0; }
                 }
-                if (has_pred) {   // predict_features with feature noise
-                    uint32_t w[4];
-                    philox_rk((uint32_t)s, (uint32_t)j, (uint32_t)p, ctr_word3(pred_frame, ST_FEAT, 0), prm.rk, w);
-                    T z[4];
-                    Pair<T>::two(w[0], w[1], z[0], z[1]);
-                    Pair<T>::two(w[2], w[3], z[2], z[3]);
+                const bool inr = valid && in_range(y, m);
+                const T pds = inr ? (T)m.pd : T(0);
+                n_in += __popc(__ballot_sync(0xffffffffu, inr) & (g ? 0xffff0000u : 0x0000ffffu));
+                if (!raw && valid && wnd) {   // non-detection cloud candidate: predicted world point, weight 1 - pD
+                    T* cl_out = b.cloud[cur ^ 1] + ((size_t)p * prm.Gcap + j) * 7 * Ps;
 #pragma unroll
-                    for (int q = 0; q < 3; ++q) {
-                        T a2 = (T)prm.feat_std[q] * z[q];
-                        X[q] = X[q] + X[q + 3] * dtT + a2 * half_dt2;
-                        X[q + 3] = X[q + 3] + a2 * dtT;
+                    for (int a2 = 0; a2 < 6; ++a2) __stcs(cl_out + a2 * Ps + s, X[a2]);
+                    __stcs(cl_out + 6 * Ps + s, T(1) - pds);
+                }
+                const T wp = om * pds;
+                any |= wp != T(0);
+                if (t == 0) {   // shift: the Gaussian's first sample (lane 0 or 16), if finite, else 0
+#pragma unroll
+                    for (int a2 = 0; a2 < 6; ++a2) {
+                        const T v = __shfl_sync(0xffffffffu, y[a2], lane & 16);
+                        shift[a2] = isfinite(v) ? v : T(0);
+                    }
+                    if (hl < 6 && gvalid) shift_g[hl] = shift[hl];
+                }
+                if (stage && gvalid && s < P4) {
+                    if (raw) {
+#pragma unroll
+                        for (int a2 = 0; a2 < 6; ++a2) Y[a2 * sY + s] = y[a2];
+                    } else {   // r d and r = sqrt(w'); zero-weight samples (and the padding) stage zeros
+                        const T r = wp != T(0) ? tsqrt(wp) : T(0);
+#pragma unroll
+                        for (int a2 = 0; a2 < 6; ++a2) Y[a2 * sY + s] = wp != T(0) ? r * (y[a2] - shift[a2]) : T(0);
+                        Y[6 * sY + s] = r;
+                        Y[7 * sY + s] = wp;
                     }
                 }
-                measure(X, pose_upd, m, y);
-            } else {
-#pragma unroll
-                for (int a2 = 0; a2 < 6; ++a2) { X[a2] = 0; y[a2] = 0; }
             }
-            const bool inr = valid && in_range(y, m);
-            const T pds = inr ? (T)m.pd : T(0);
-            const unsigned in_mask = __ballot_sync(0xffffffffu, inr);
-            const unsigned g_mask = __ballot_sync(0xffffffffu, valid && g == 1);
-            n_in0 += __popc(in_mask & ~g_mask);
-            n_in1 += __popc(in_mask & g_mask);
-            if (valid && (g ? wnd1 : wnd0)) {   // non-detection cloud candidate: predicted world point, weight 1 - pD
-                T* cl_out = b.cloud[cur ^ 1] + ((size_t)p * prm.Gcap + j) * 7 * Ps;
-#pragma unroll
-                for (int a2 = 0; a2 < 6; ++a2) __stcs(cl_out + a2 * Ps + s, X[a2]);
-                __stcs(cl_out + 6 * Ps + s, T(1) - pds);
-            }
-            const T wp = om * pds;
-            if (g) any1 |= wp != T(0);
-            else any0 |= wp != T(0);
-            if (valid) {   // staged as measured; the shift is taken per Gaussian below
-                T* Y = Ywarp + (size_t)g * kStageRows * sY;
-#pragma unroll
-                for (int a2 = 0; a2 < 6; ++a2) Y[a2 * sY + s] = y[a2];
-                Y[6 * sY + s] = wp;
-            }
-        }
-        if (lane == 0) atomicAdd(&s_wr, (int)wnd0 + (nG > 1 ? (int)wnd1 : 0));
-        any0 = __any_sync(0xffffffffu, any0);
-        any1 = __any_sync(0xffffffffu, any1);
-        __syncwarp();
-        for (int g = 0; g < nG; ++g) {
-            const int j = j0 + g;
-            const T W = g ? Wg[1] : Wg[0];
-            T* Y = Ywarp + (size_t)g * kStageRows * sY;
-            const bool any_w = g ? any1 : any0;
-            const T pbar = (T)((double)(g ? n_in1 : n_in0) * m.pd / (double)P);
-            T shift[6];   // the Gaussian's first sample, if finite, else 0
-#pragma unroll
-            for (int a2 = 0; a2 < 6; ++a2) {
-                const T v = Y[a2 * sY];
-                shift[a2] = isfinite(v) ? v : T(0);
-            }
+        };
+        sample_pass(false, true);
+        if (lane == 0) atomicAdd(&s_wr, (int)(Wg[0] >= (T)prm.min_weight) + (nG > 1 ? (int)(Wg[1] >= (T)prm.min_weight) : 0));
+        const bool any0 = __any_sync(0xffffffffu, any && g == 0), any1 = __any_sync(0xffffffffu, any && g == 1);
+        const int n_in0 = __shfl_sync(0xffffffffu, n_in, 0), n_in1 = __shfl_sync(0xffffffffu, n_in, 16);
+        // the fallback fit (below) needs the raw samples: rare, so they are drawn again
+        const bool raw0 = !any0 && n_in0 > 0 && m.pd > 0.0, raw1 = nG > 1 && !any1 && n_in1 > 0 && m.pd > 0.0;
+        if (raw0 || raw1) {
             __syncwarp();
+            sample_pass(true, g ? raw1 : raw0);
+        }
+        __syncwarp();
+        for (int gg = 0; gg < nG; ++gg) {
+            const int jj = j0 + gg;
+            const T W = gg ? Wg[1] : Wg[0];
+            const T* Yg = Ywarp + (size_t)gg * (kStageRows * sY + 16);
+            const T* sh = s_shift + (warp * 2 + gg) * 6;
+            const bool any_w = gg ? any1 : any0;
+            const T pbar = (T)((double)(gg ? n_in1 : n_in0) * m.pd / (double)P);
             if (any_w) {
-                // d = y - shift; zero-weight samples (and the padding) leave the sums
-                for (int s = lane; s < P4; s += 32) {
-                    const T w = s < P ? Y[6 * sY + s] : T(0);
-#pragma unroll
-                    for (int a2 = 0; a2 < 6; ++a2) Y[a2 * sY + s] = w != T(0) ? Y[a2 * sY + s] - shift[a2] : T(0);
-                    if (s >= P) Y[6 * sY + s] = T(0);
-                }
-                __syncwarp();
                 // lane q < 29: moment q over the samples, four partial sums
-                const T mom = lane < 29 ? moment_sweep(Y + 6 * sY, Y + ra * sY, Y + rb * sY, P4) : T(0);
+                const T mom = lane < 29 ? moment_sweep(Yg + ra * sY, Yg + rb * sY, P4) : T(0);
                 const T S0 = __shfl_sync(0xffffffffu, mom, 0), S2 = __shfl_sync(0xffffffffu, mom, 1);
                 const T inv = T(1) / S0, scale = T(1) + S2 * inv * inv;
                 // lanes 2-7 hold S1 (the mean offsets), lanes 8-28 hold SS
@@ -433,14 +445,14 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
                     if (ra == a2) da = dvals[a2];
                     if (rb == a2) db = dvals[a2];
                 }
-                if (lane >= 2 && lane < 8) fitw[lane] = shift[lane - 2] + dl;
+                if (lane >= 2 && lane < 8) fitw[lane] = sh[lane - 2] + dl;
                 if (lane >= 8 && lane < 29) fitw[lane] = (mom * inv - da * db) * scale;
             } else if (pbar > T(0)) {
                 // every sample weighted 1 (exp(LOG0 - LOG0)): unnormalised mean (sum of the
-                // samples) and covariance x (P + P)/P over the valid samples
+                // samples) and covariance x (P + P)/P over the valid samples (raw rows)
                 T mu = 0;
                 if (lane < 6) {
-                    for (int s = 0; s < P; ++s) mu += Y[lane * sY + s];
+                    for (int s = 0; s < P; ++s) mu += Yg[lane * sY + s];
                 }
                 T mus[6];
 #pragma unroll
@@ -453,20 +465,20 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
                         if (ra == a2) ma = mus[a2];
                         if (rb == a2) mb = mus[a2];
                     }
-                    for (int s = 0; s < P; ++s) cva += (Y[ra * sY + s] - ma) * (Y[rb * sY + s] - mb);
+                    for (int s = 0; s < P; ++s) cva += (Yg[ra * sY + s] - ma) * (Yg[rb * sY + s] - mb);
                 }
                 const T scale = (T(P) * T(P) + T(P)) / T(P);
                 if (lane < 6) fitw[2 + lane] = mu;
                 if (lane >= 8 && lane < 29) fitw[lane] = cva * scale;
             } else {   // entirely out of view: never used downstream (its log-constant is -inf)
-                if (lane < 6) fitw[2 + lane] = shift[lane];
+                if (lane < 6) fitw[2 + lane] = sh[lane];
                 if (lane >= 8 && lane < 29) fitw[lane] = T(0);
             }
             if (lane == 0) fitw[0] = W;
             if (lane == 1) fitw[1] = pbar;
             __syncwarp();
             // fitted row: lane q writes element q (W, pD, mean[6], packed cov[21])
-            T* fr = b.fit + ((size_t)p * prm.Gcap + j) * kRow;
+            T* fr = b.fit + ((size_t)p * prm.Gcap + jj) * kRow;
             if (lane < 29) fr[lane] = fitw[lane];
             __syncwarp();
         }
