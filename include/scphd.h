@@ -169,7 +169,9 @@ scphd_status scphd_set_state(scphd_filter* f, const double* states, const double
  * [7] survivors since create, [8] sample clouds read from memory, [9] sample
  * clouds written, [10] Gaussians fitted, [11] merged components produced,
  * [12] full Mahalanobis evaluations in the merge, [13] largest survivor count of
- * one parent (before the max_survivors cut); [14..15] reserved. */
+ * one parent (before the max_survivors cut), [14] Gaussians fitted with unit sample
+ * weights (in view, but every in-view sample of zero weight: only with pd = 1);
+ * [15] reserved. */
 scphd_status scphd_get_counters(scphd_filter* f, int64_t counters[16]);
 
 /* Launch shapes tuned on the filter's first updates that have measurements: threads

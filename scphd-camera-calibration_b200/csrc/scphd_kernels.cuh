@@ -470,6 +470,7 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
                 const T scale = (T(P) * T(P) + T(P)) / T(P);
                 if (lane < 6) fitw[2 + lane] = mu;
                 if (lane >= 8 && lane < 29) fitw[lane] = cva * scale;
+                if (lane == 0) atomicAdd(&b.counters[14], 1ull);
             } else {   // entirely out of view: never used downstream (its log-constant is -inf)
                 if (lane < 6) fitw[2 + lane] = sh[lane];
                 if (lane >= 8 && lane < 29) fitw[lane] = T(0);

@@ -88,8 +88,8 @@ def test_fp64_frames_match_oracle(pkg, orc, meas_dim):
 
 @pytest.mark.parametrize("particles", [7, 33])
 def test_fp64_frames_match_oracle_sample_counts(pkg, orc, particles):
-    """Sample counts where the two Gaussians a warp samples together meet inside one
-    32-lane iteration (P < 32) or one lane past it (P = 33)."""
+    """Sample counts that leave a 16-sample pass of a half-warp partly filled (P = 7)
+    or reach one sample into a third pass (P = 33), both padded to 4-sample rows."""
     _need_gpu()
     sc = pkg.scene.make_scene(n_landmarks=16, n_frames=6, clutter_rate=4.0, seed=pkg.scene.scene_seed(0, 12))
     cfg = pkg.scene.filter_config(n_parents=24, max_gaussians=160, max_meas=96, clutter_rate=4.0,
@@ -103,6 +103,27 @@ def test_fp64_frames_match_oracle_sample_counts(pkg, orc, particles):
             f.update(z[:, 0], z[:, 1], fixed_camera=sc.fixed[k], d=z[:, 2])
         _compare_frame(gpu, ref, z.shape[0], k)
         assert gpu.resample() == ref.resample(), f"frame {k} resample decision"
+
+
+def test_fp64_frames_match_oracle_certain_detection(pkg, orc):
+    """pd = 1: a non-detection cloud's in-view samples carry weight 1 - pd = 0, so a
+    cloud whose out-of-view samples stay out of view has all in-view weights 0 and is
+    fitted with unit weights (the reference's fallback), from samples drawn again."""
+    _need_gpu()
+    # a scene (searched with the oracle) where such fits occur in frames 3, 5 and 7
+    sc = pkg.scene.make_scene(n_landmarks=20, n_frames=8, clutter_rate=4.0, seed=pkg.scene.scene_seed(0, 27))
+    cfg = pkg.scene.filter_config(n_parents=32, max_gaussians=160, max_meas=96, clutter_rate=4.0,
+                                  precision=pkg.SCPHD_FP64, calib=sc.calib, seed=27, particles_per_feature=40)
+    cfg.pd = 1.0
+    gpu, ref = _pair(pkg, orc, cfg)
+    for k in range(sc.n_frames):
+        z = sc.frames[k]
+        for f in (gpu, ref):
+            f.predict(pkg.scene.DT)
+            f.update(z[:, 0], z[:, 1], fixed_camera=sc.fixed[k], d=z[:, 2])
+        _compare_frame(gpu, ref, z.shape[0], k)
+        assert gpu.resample() == ref.resample(), f"frame {k} resample decision"
+    assert gpu.counters()[14] > 0, "no Gaussian took the unit-weight fit"
 
 
 def test_reference_fixture_frames(pkg, orc):
