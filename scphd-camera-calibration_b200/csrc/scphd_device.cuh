@@ -261,6 +261,66 @@ __device__ inline bool chol6(const T* A, T* L) {
     return ok;
 }
 
+// FP32 form of the factorisation: each pivot's reciprocal square root is taken once
+// and the column below the pivot is scaled by it (hardware rsqrt, max 2 ulp), in the
+// same order.  A pivot <= 0 gives NaN (0 * inf, or the rsqrt of a negative number): the
+// PD outcome is the division form's, except that an exactly zero last pivot also
+// reports not PD.  The FP64 form keeps the square roots and divisions.
+template <>
+__device__ inline bool chol6<float>(const float* A, float* L) {
+    float inv[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+#pragma unroll
+        for (int j = 0; j <= i; ++j) {
+            float tmp = A[tri(i, j)];
+            if (i == j) {
+#pragma unroll
+                for (int k = 0; k < j; ++k) tmp -= L[tri(j, k)] * L[tri(j, k)];
+                inv[i] = rsqrtf(tmp);
+                L[tri(i, i)] = tmp * inv[i];
+            } else {
+#pragma unroll
+                for (int k = 0; k < j; ++k) tmp -= L[tri(i, k)] * L[tri(j, k)];
+                L[tri(i, j)] = tmp * inv[j];
+            }
+        }
+    }
+    bool ok = true;
+#pragma unroll
+    for (int i = 0; i < 21; ++i) ok = ok && !isnan(L[i]);
+    return ok;
+}
+
+// A map or merge row's 28 leading values (weight, mean[6], packed 6x6[21]) in 16-byte
+// pieces; rows start 16-byte aligned (kRow values apart from an aligned base).
+__device__ __forceinline__ void row28_load(const float* src, float v[28]) {
+    const float4* q = reinterpret_cast<const float4*>(src);
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+        const float4 x = q[i];
+        v[4 * i] = x.x; v[4 * i + 1] = x.y; v[4 * i + 2] = x.z; v[4 * i + 3] = x.w;
+    }
+}
+__device__ __forceinline__ void row28_load(const double* src, double v[28]) {
+    const double2* q = reinterpret_cast<const double2*>(src);
+#pragma unroll
+    for (int i = 0; i < 14; ++i) {
+        const double2 x = q[i];
+        v[2 * i] = x.x; v[2 * i + 1] = x.y;
+    }
+}
+__device__ __forceinline__ void row28_store(float* dst, const float v[28]) {
+    float4* q = reinterpret_cast<float4*>(dst);
+#pragma unroll
+    for (int i = 0; i < 7; ++i) q[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+}
+__device__ __forceinline__ void row28_store(double* dst, const double v[28]) {
+    double2* q = reinterpret_cast<double2*>(dst);
+#pragma unroll
+    for (int i = 0; i < 14; ++i) q[i] = make_double2(v[2 * i], v[2 * i + 1]);
+}
+
 // PD test of an update's posterior covariance: a Cholesky whose every pivot exceeds
 // 1e-10 of its diagonal entry.  Unlike the reference's isPosDef (no NaN in the factor),
 // an exactly singular posterior -- after a refit from fewer in-view samples than

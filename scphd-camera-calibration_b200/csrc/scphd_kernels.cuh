@@ -1064,17 +1064,14 @@ __device__ void merge_members_thread(const View& v, const T* s_w, const int* mem
     for (int e = 0; e < 21; ++e) row[7 + e] = cv[e] / W;
     T L[21];
     const bool pd = chol6(row + 7, L);
-    T* o = sparse + (size_t)c * kRow;
-    if (pd) {
+    if (!pd) {   // "bad hack, just keep the max feature" (kernels.cu:855-862)
+        row[0] = s_w[c];
 #pragma unroll
-        for (int q = 0; q < 28; ++q) o[q] = row[q];
-    } else {   // "bad hack, just keep the max feature" (kernels.cu:855-862)
-        o[0] = s_w[c];
+        for (int a = 0; a < 6; ++a) row[1 + a] = cmu[a];
 #pragma unroll
-        for (int a = 0; a < 6; ++a) o[1 + a] = cmu[a];
-#pragma unroll
-        for (int e = 0; e < 21; ++e) o[7 + e] = ccov[e];
+        for (int e = 0; e < 21; ++e) row[7 + e] = ccov[e];
     }
+    row28_store(sparse + (size_t)c * kRow, row);
 }
 
 // Order-preserving integer key of a non-negative weight.
@@ -1567,13 +1564,13 @@ __device__ __forceinline__ void merge_body(const Params& prm, const Bufs<T>& b, 
         const int nxt = (e + 1 < n_all) ? s_pos[e + 1] : total;
         if (nxt == pos) continue;   // not kept
         if (e < n_out) {   // merged component: weight, mean and the Cholesky factor of its covariance
-            const T* sr = sparse + (size_t)centre_of[e] * kRow;
+            T v[28];
+            row28_load(sparse + (size_t)centre_of[e] * kRow, v);
             T L[21];
-            chol6(sr + 7, L);
-            T* dr = mo + (size_t)pos * kRow;
-            for (int q = 0; q < 7; ++q) dr[q] = sr[q];
+            chol6(v + 7, L);
 #pragma unroll
-            for (int q = 0; q < 21; ++q) dr[7 + q] = L[q];
+            for (int q = 0; q < 21; ++q) v[7 + q] = L[q];
+            row28_store(mo + (size_t)pos * kRow, v);
             mr[pos] = -1 - e;
         } else {
             const int j = e - n_out;
