@@ -292,6 +292,12 @@ __device__ inline bool chol6<float>(const float* A, float* L) {
     return ok;
 }
 
+// x / w for a moment-matched merge's normalisation by its weight w (inv = 1 / w): in
+// FP32 the product with the reciprocal (within 1.5 ulp of the quotient), in FP64 the
+// correctly rounded quotient.
+__device__ __forceinline__ float div_by(float x, float w, float inv) { (void)w; return x * inv; }
+__device__ __forceinline__ double div_by(double x, double w, double inv) { (void)inv; return x / w; }
+
 // A map or merge row's 28 leading values (weight, mean[6], packed 6x6[21]) in 16-byte
 // pieces; rows start 16-byte aligned (kRow values apart from an aligned base).
 __device__ __forceinline__ void row28_load(const float* src, float v[28]) {

@@ -1038,8 +1038,9 @@ __device__ void merge_members_thread(const View& v, const T* s_w, const int* mem
     }
     T row[28];
     row[0] = W;
+    const T iW = T(1) / W;
 #pragma unroll
-    for (int a = 0; a < 6; ++a) row[1 + a] = acc[a] / W;
+    for (int a = 0; a < 6; ++a) row[1 + a] = div_by(acc[a], W, iW);
     T cv[21];
 #pragma unroll
     for (int e = 0; e < 21; ++e) cv[e] = 0;
@@ -1061,7 +1062,7 @@ __device__ void merge_members_thread(const View& v, const T* s_w, const int* mem
             for (int bb = 0; bb <= a; ++bb) cv[tri(a, bb)] += w * (sc[tri(a, bb)] + d[a] * d[bb]);
     }
 #pragma unroll
-    for (int e = 0; e < 21; ++e) row[7 + e] = cv[e] / W;
+    for (int e = 0; e < 21; ++e) row[7 + e] = div_by(cv[e], W, iW);
     T L[21];
     const bool pd = chol6(row + 7, L);
     if (!pd) {   // "bad hack, just keep the max feature" (kernels.cu:855-862)
