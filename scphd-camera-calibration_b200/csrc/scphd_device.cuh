@@ -292,9 +292,16 @@ __device__ inline bool chol6<float>(const float* A, float* L) {
     return ok;
 }
 
-// x / w for a moment-matched merge's normalisation by its weight w (inv = 1 / w): in
-// FP32 the product with the reciprocal (within 1.5 ulp of the quotient), in FP64 the
-// correctly rounded quotient.
+// sqrt(w) of a sample weight w > 0 for the moment rows: in FP32 w rsqrt(w) for normal
+// w (max 2 ulp; the rows only need r r = w to a few ulp), else the square root
+__device__ __forceinline__ float weight_root(float w) {
+    if (w >= 1.17549435e-38f) return w * rsqrtf(w);
+    return sqrtf(w);
+}
+__device__ __forceinline__ double weight_root(double w) { return sqrt(w); }
+
+// x / w where one w divides several values (inv = 1 / w): in FP32 the product with the
+// reciprocal (within 1.5 ulp of the quotient), in FP64 the correctly rounded quotient.
 __device__ __forceinline__ float div_by(float x, float w, float inv) { (void)w; return x * inv; }
 __device__ __forceinline__ double div_by(double x, double w, double inv) { (void)inv; return x / w; }
 
@@ -348,6 +355,35 @@ __device__ inline bool posterior_pd(const T* A) {
 #pragma unroll
                 for (int k = 0; k < j; ++k) tmp -= L[tri(i, k)] * L[tri(j, k)];
                 L[tri(i, j)] = tmp / L[tri(j, j)];
+            }
+        }
+    }
+    bool ok = true;
+#pragma unroll
+    for (int i = 0; i < 21; ++i) ok = ok && !isnan(L[i]);
+    return ok;
+}
+
+// FP32 form of the same test: one rsqrt per pivot, the column scaled by it (max 2 ulp);
+// the pivot test is the same comparison.
+template <>
+__device__ inline bool posterior_pd<float>(const float* A) {
+    float L[21], inv[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+#pragma unroll
+        for (int j = 0; j <= i; ++j) {
+            float tmp = A[tri(i, j)];
+            if (i == j) {
+#pragma unroll
+                for (int k = 0; k < j; ++k) tmp -= L[tri(j, k)] * L[tri(j, k)];
+                if (!(tmp > 1e-10f * A[tri(i, i)])) return false;
+                inv[i] = rsqrtf(tmp);
+                L[tri(i, i)] = tmp * inv[i];
+            } else {
+#pragma unroll
+                for (int k = 0; k < j; ++k) tmp -= L[tri(i, k)] * L[tri(j, k)];
+                L[tri(i, j)] = tmp * inv[j];
             }
         }
     }
@@ -453,7 +489,8 @@ __device__ inline void kalman_prep(T w, T pdbar, const T* P, const Model& m, T* 
     T det;
     if (K == 2) {
         det = S[0] * S[2] - S[1] * S[1];
-        Si[0] = S[2] / det; Si[1] = -S[1] / det; Si[2] = S[0] / det;
+        const T idet = T(1) / det;
+        Si[0] = div_by(S[2], det, idet); Si[1] = div_by(-S[1], det, idet); Si[2] = div_by(S[0], det, idet);
         Si[3] = Si[4] = Si[5] = 0;
     } else {
         S[3] = P[3]; S[4] = P[4]; S[5] = P[5] + (T)m.var[2];
@@ -461,8 +498,9 @@ __device__ inline void kalman_prep(T w, T pdbar, const T* P, const Model& m, T* 
         T A00 = c * f - e * e, A10 = d * e - b * f, A11 = a * f - d * d;
         T A20 = b * e - c * d, A21 = b * d - a * e, A22 = a * c - b * b;
         det = a * A00 + b * A10 + d * A20;
-        Si[0] = A00 / det; Si[1] = A10 / det; Si[2] = A11 / det;
-        Si[3] = A20 / det; Si[4] = A21 / det; Si[5] = A22 / det;
+        const T idet = T(1) / det;
+        Si[0] = div_by(A00, det, idet); Si[1] = div_by(A10, det, idet); Si[2] = div_by(A11, det, idet);
+        Si[3] = div_by(A20, det, idet); Si[4] = div_by(A21, det, idet); Si[5] = div_by(A22, det, idet);
     }
     const T log2pi = (T)1.8378770664093454835606594728112;
     T cst;

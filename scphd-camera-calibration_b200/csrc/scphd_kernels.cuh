@@ -402,7 +402,7 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
 #pragma unroll
                         for (int a2 = 0; a2 < 6; ++a2) Y[a2 * sY + s] = y[a2];
                     } else {   // r d and r = sqrt(w'); zero-weight samples (and the padding) stage zeros
-                        const T r = wp != T(0) ? tsqrt(wp) : T(0);
+                        const T r = wp != T(0) ? weight_root(wp) : T(0);
 #pragma unroll
                         for (int a2 = 0; a2 < 6; ++a2) Y[a2 * sY + s] = wp != T(0) ? r * (y[a2] - shift[a2]) : T(0);
                         Y[6 * sY + s] = r;
