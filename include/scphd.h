@@ -50,7 +50,7 @@ enum { SCPHD_FP32 = 0, SCPHD_FP64 = 1 };
  * precision and seed are additions of this implementation. */
 typedef struct scphd_config {
     int32_t n_parents;              /* n_particles */
-    int32_t particles_per_feature;  /* Monte-Carlo samples per daughter Gaussian, <= 256 (<= 212 in FP64) */
+    int32_t particles_per_feature;  /* Monte-Carlo samples per daughter Gaussian, <= 256 (<= 216 in FP64) */
     int32_t max_gaussians;          /* per-parent map capacity (G_max) */
     int32_t max_measurements;       /* per-frame measurement capacity (M_max) */
     int32_t meas_dim;               /* 2: (u,v) as the reference; 3: (u,v,d) */

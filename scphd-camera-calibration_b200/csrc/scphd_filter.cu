@@ -274,7 +274,7 @@ public:
         fit_smem = cloud_fit_smem_bytes<T>(prm.P);
         if (fit_smem > 220 * 1024)   // with the kernel's static shared memory, within 227 KB per block
             return fail(SCPHD_ERR_CAPACITY, "particles_per_feature needs " + std::to_string(fit_smem) +
-                                                " bytes of shared memory per cloud-fit block (FP64 allows up to 212)");
+                                                " bytes of shared memory per cloud-fit block (FP64 allows up to 216)");
         if (merge_smem > 227 * 1024)
             return fail(SCPHD_ERR_CAPACITY, "max_survivors/max_gaussians need " + std::to_string(merge_smem) +
                                                 " bytes of shared memory per merge block (limit 227 KB)");

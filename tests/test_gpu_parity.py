@@ -105,6 +105,38 @@ def test_fp64_frames_match_oracle_sample_counts(pkg, orc, particles):
         assert gpu.resample() == ref.resample(), f"frame {k} resample decision"
 
 
+def test_fp64_largest_sample_count_matches_oracle(pkg, orc):
+    """216 samples per Gaussian, the most whose FP64 sample rows fit one cloud-fit
+    block's shared memory; 217 is refused at create, as is more than 256 in FP32."""
+    _need_gpu()
+    sc = pkg.scene.make_scene(n_landmarks=12, n_frames=4, clutter_rate=3.0, seed=pkg.scene.scene_seed(0, 14))
+    cfg = pkg.scene.filter_config(n_parents=8, max_gaussians=64, max_meas=64, clutter_rate=3.0,
+                                  precision=pkg.SCPHD_FP64, calib=sc.calib, seed=14, particles_per_feature=216)
+    gpu, ref = _pair(pkg, orc, cfg)
+    for k in range(sc.n_frames):
+        z = sc.frames[k]
+        for f in (gpu, ref):
+            f.predict(pkg.scene.DT)
+            f.update(z[:, 0], z[:, 1], fixed_camera=sc.fixed[k], d=z[:, 2])
+        _compare_frame(gpu, ref, z.shape[0], k)
+        assert gpu.resample() == ref.resample(), f"frame {k} resample decision"
+    big = cfg.copy()
+    big.particles_per_feature = 217
+    with pytest.raises(pkg.ScphdError) as e:
+        pkg.SCPHDCameraCalibration(big)
+    assert e.value.status == 3
+    fp32 = cfg.copy()
+    fp32.precision = pkg.SCPHD_FP32
+    fp32.particles_per_feature = 256
+    f = pkg.SCPHDCameraCalibration(fp32)
+    z = sc.frames[0]
+    f.step(pkg.scene.DT, z[:, 0], z[:, 1], fixed_camera=sc.fixed[0], d=z[:, 2])
+    f.checkStuff()
+    fp32.particles_per_feature = 257
+    with pytest.raises(pkg.ScphdError):
+        pkg.SCPHDCameraCalibration(fp32)
+
+
 def test_fp64_frames_match_oracle_certain_detection(pkg, orc):
     """pd = 1: a non-detection cloud's in-view samples carry weight 1 - pd = 0, so a
     cloud whose out-of-view samples stay out of view has all in-view weights 0 and is
