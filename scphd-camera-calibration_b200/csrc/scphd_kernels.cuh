@@ -599,8 +599,8 @@ __device__ __forceinline__ void likelihood_body(const Params& prm, const Bufs<T>
             // non-PD posteriors carry weight LOG0 before the normaliser (kernels.cu:597-598)
             if (!(c > tneg_inf<T>()) || t[1] == T(0)) continue;
             const T lt = log_term<T, K>(c, t + 2, t + 8, zm);
-            if (lt > mx) { acc = acc * texp(mx - lt) + T(1); mx = lt; }   // online log-sum-exp
-            else acc += texp(lt - mx);
+            if (lt > mx) { acc = acc * texp_sum(mx - lt) + T(1); mx = lt; }   // online log-sum-exp
+            else acc += texp_sum(lt - mx);
             if (lt >= cand_min) {
                 if (n_cand < kLikCand) s_cand[n_cand * blockDim.x + threadIdx.x] = k;
                 ++n_cand;
@@ -626,7 +626,7 @@ __device__ __forceinline__ void likelihood_body(const Params& prm, const Bufs<T>
             load_terms(s_terms + (size_t)k * kLikTerms, t);
             const T c = t[0];
             if (!(c > tneg_inf<T>() && t[1] > T(0))) continue;
-            const T w = texp(log_term<T, K>(c, t + 2, t + 8, zm) - ell);
+            const T w = texp_sum(log_term<T, K>(c, t + 2, t + 8, zm) - ell);
             if (w >= minw) {
                 const int slot = atomicAdd(&b.surv_n[p], 1);
                 if (slot < prm.Scap) {
