@@ -142,12 +142,6 @@ template <typename T> __device__ __forceinline__ T tneg_inf();
 template <> __device__ __forceinline__ float tneg_inf() { return -INFINITY; }
 template <> __device__ __forceinline__ double tneg_inf() { return -INFINITY; }
 
-template <typename T> __device__ __forceinline__ T warp_sum(T v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
 // ------------------------------------------------------------------ camera model
 // Rotation terms of the reference's world<->camera transform
 // (src/disparitymeasurementmodel.cu:3-144), evaluated once per parent in FP64.

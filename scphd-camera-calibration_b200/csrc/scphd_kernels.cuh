@@ -1082,7 +1082,7 @@ __device__ __forceinline__ uint64_t weight_key(double w) { return (uint64_t)__do
 // Exact k-th largest key among the entries with w >= 0 (k <= their count), by an
 // MSB-first radix select over 8-bit digits.  Block-wide call.
 template <typename T>
-__device__ uint64_t select_kth_largest(const T* w, int n, int k, int* s_tmp) {
+__device__ uint64_t select_kth_largest(const T* w, int n, int k) {
     __shared__ int s_hist[256];
     __shared__ uint64_t s_prefix;
     __shared__ int s_k;
@@ -1129,7 +1129,6 @@ __device__ uint64_t select_kth_largest(const T* w, int n, int k, int* s_tmp) {
         prefix = s_prefix;
         mask |= (uint64_t)255 << (8 * d);
     }
-    (void)s_tmp;
     return prefix;
 }
 
@@ -1532,7 +1531,7 @@ __device__ __forceinline__ void merge_body(const Params& prm, const Bufs<T>& b, 
         for (int e = tid; e < n_all; e += blockDim.x) s_pos[e] = s_w[e] >= T(0);
         __syncthreads();
     } else {
-        const uint64_t thr = select_kth_largest(s_w, n_all, prm.Gcap, s_tmp);
+        const uint64_t thr = select_kth_largest(s_w, n_all, prm.Gcap);
         // entries above the threshold, then ties in entry order up to Gcap
         int above = 0;
         for (int e = tid; e < n_all; e += blockDim.x) {
