@@ -786,6 +786,25 @@ struct KeyItems {   // (key, value) by ascending key
     }
 };
 
+// FP32 survivors as one 64-bit key each, sorted descending: the weight's bits (a
+// non-negative float orders as its bit pattern) above the complement of the tie key,
+// so that the order is merge_before's; padding slots hold 0 and sort last.  Half the
+// shuffles and a single compare per exchange against SurvItems.
+struct PackedSurvItems {
+    unsigned long long* k;
+    typedef unsigned long long Item;
+    __device__ Item load(int i) const { return k[i]; }
+    __device__ void store(int i, const Item& x) const { k[i] = x; }
+    __device__ static bool before(const Item& a, const Item& b) { return a > b; }
+    __device__ static Item shfl(const Item& x, int m) { return __shfl_xor_sync(0xffffffffu, x, m); }
+};
+__device__ __forceinline__ unsigned long long pack_survivor(float w, uint32_t r) {
+    return ((unsigned long long)__float_as_uint(w) << 32) | (uint32_t)~tie_key(r);
+}
+__device__ __forceinline__ uint32_t untie_key(uint32_t t) {   // inverse of tie_key
+    return ((t & 0xffffffu) << 8) | (__brev(t >> 24) >> 24);
+}
+
 // one shared-memory stage (k, j) over all pairs
 template <typename Items>
 __device__ __forceinline__ void bitonic_smem_stage(const Items& it, int n_pad, int k, int jj) {
@@ -1428,8 +1447,15 @@ __device__ __forceinline__ void merge_body(const Params& prm, const Bufs<T>& b, 
     MergeScratch<T> ms;
     carve_merge_smem<T>(smem, prm.Scap, prm.Gcap, true, s_w, s_key, s_r, s_pos, ms);
     __shared__ int s_tmp[40];
+    // FP32: packed sort keys in the survivor staging area (free until the survivors are
+    // staged; 8 n_pad <= 16 Scap bytes fit in its 28 Scap); FP64: (weight, tie key, rank)
+    unsigned long long* s_pk = reinterpret_cast<unsigned long long*>(smem);
     for (int i = tid; i < n_pad; i += blockDim.x) {
-        if (i < n) {
+        if (sizeof(T) == 4) {
+            s_pk[i] = i < n ? pack_survivor((float)b.surv_w[(size_t)p * prm.Scap + i],
+                                            (uint32_t)b.surv_r[(size_t)p * prm.Scap + i])
+                            : 0ull;
+        } else if (i < n) {
             s_w[i] = b.surv_w[(size_t)p * prm.Scap + i];
             s_r[i] = b.surv_r[(size_t)p * prm.Scap + i];
             s_key[i] = tie_key((uint32_t)s_r[i]);
@@ -1453,7 +1479,17 @@ __device__ __forceinline__ void merge_body(const Params& prm, const Bufs<T>& b, 
         for (int w2 = 0; w2 < (int)(blockDim.x >> 5); ++w2) t += s_red[w2];
         b.loglik[p] = t;
     }
-    sort_survivors(s_w, s_key, s_r, n_pad);
+    if (sizeof(T) == 4) {
+        block_bitonic_sort(PackedSurvItems{s_pk}, n_pad);
+        for (int i = tid; i < n_pad; i += blockDim.x) {
+            const unsigned long long v = s_pk[i];
+            s_w[i] = i < n ? (T)__uint_as_float((uint32_t)(v >> 32)) : T(-1);
+            s_r[i] = i < n ? (int)untie_key(~(uint32_t)v) : 0x7fffffff;
+        }
+        __syncthreads();   // the staging below reuses the key area
+    } else {
+        sort_survivors(s_w, s_key, s_r, n_pad);
+    }
     KalmanSource<T, K> src;
     src.fit = b.fit + (size_t)p * prm.Gcap * kRow;
     src.prep = b.prep + (size_t)p * prm.Gcap * kPrep;
