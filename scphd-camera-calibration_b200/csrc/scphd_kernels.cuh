@@ -568,11 +568,17 @@ __device__ __forceinline__ void likelihood_body(const Params& prm, const Bufs<T>
                                                 int mblock, T* s_terms) {
     const int m = mblock * blockDim.x + threadIdx.x;
     const int G = min(b.map_n[cur][b.src[p]], prm.Gcap);
-    for (int jj = threadIdx.x; jj < G; jj += blockDim.x) {   // per Gaussian: c, pD flag, S^-1, mean, pad
+    // per Gaussian: c, pD flag, S^-1, mean, pad; a non-PD posterior's c is staged as -inf
+    // (its weight is LOG0 before the normaliser, kernels.cu:597-598), so that the
+    // normaliser pass needs no test
+    T cm = tneg_inf<T>();
+    for (int jj = threadIdx.x; jj < G; jj += blockDim.x) {
         const T* pr = b.prep + ((size_t)p * prm.Gcap + jj) * kPrep;
         const T* fr = b.fit + ((size_t)p * prm.Gcap + jj) * kRow;
         T* t = s_terms + (size_t)jj * kLikTerms;
-        t[0] = pr[0];
+        const T c = (pr[0] > tneg_inf<T>() && pr[1] != T(0)) ? pr[0] : tneg_inf<T>();
+        cm = c > cm ? c : cm;
+        t[0] = c;
         t[1] = pr[1];
 #pragma unroll
         for (int i = 0; i < 6; ++i) t[2 + i] = pr[kPrepSi + i];
@@ -589,26 +595,57 @@ __device__ __forceinline__ void likelihood_body(const Params& prm, const Bufs<T>
     const T cand_min = bpc + (T)log(prm.min_weight) - T(1);
     int* s_cand = reinterpret_cast<int*>(s_terms + (size_t)prm.Gcap * kLikTerms);   // [slot][thread]
     int n_cand = 0;
+    // largest log-constant of the parent: lt_j <= c_j, since the quadratic form is >= 0
+    __shared__ T s_cm[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const T v = __shfl_xor_sync(0xffffffffu, cm, o);
+        cm = v > cm ? v : cm;
+    }
+    if ((threadIdx.x & 31) == 0) s_cm[threadIdx.x >> 5] = cm;
     __syncthreads();
+    for (int w2 = 0; w2 < (int)(blockDim.x >> 5); ++w2) cm = s_cm[w2] > cm ? s_cm[w2] : cm;
+    // FP32: the sum is taken around the fixed shift s0 = max(c_max, bpc) when no term
+    // that matters can underflow there (every term within ~20 of bpc is within 80 of s0);
+    // otherwise (a log-constant far above bpc), and always in FP64, by an online
+    // log-sum-exp around the running maximum, whose dominant term is exp(0) = 1 exactly:
+    // a weight near 1 then rounds as in the FP64 oracle, and the merge order of nearly
+    // tied weights with it.
+    const T s0 = cm > bpc ? cm : bpc;
+    const bool fixed_shift = sizeof(T) == 4 && !(cm - bpc > T(60));
     T mx = tneg_inf<T>(), acc = 0;
     if (m < M) {
-        for (int k = 0; k < G; ++k) {
-            T t[kLikTerms];
-            load_terms(s_terms + (size_t)k * kLikTerms, t);
-            const T c = t[0];
-            // non-PD posteriors carry weight LOG0 before the normaliser (kernels.cu:597-598)
-            if (!(c > tneg_inf<T>()) || t[1] == T(0)) continue;
-            const T lt = log_term<T, K>(c, t + 2, t + 8, zm);
-            if (lt > mx) { acc = acc * texp_sum(mx - lt) + T(1); mx = lt; }   // online log-sum-exp
-            else acc += texp_sum(lt - mx);
-            if (lt >= cand_min) {
-                if (n_cand < kLikCand) s_cand[n_cand * blockDim.x + threadIdx.x] = k;
-                ++n_cand;
+        if (fixed_shift) {
+            for (int k = 0; k < G; ++k) {
+                T t[kLikTerms];
+                load_terms(s_terms + (size_t)k * kLikTerms, t);
+                const T lt = log_term<T, K>(t[0], t + 2, t + 8, zm);   // -inf for a non-PD posterior
+                acc += texp_sum(lt - s0);
+                if (lt >= cand_min) {
+                    if (n_cand < kLikCand) s_cand[n_cand * blockDim.x + threadIdx.x] = k;
+                    ++n_cand;
+                }
+            }
+        } else {
+            for (int k = 0; k < G; ++k) {
+                T t[kLikTerms];
+                load_terms(s_terms + (size_t)k * kLikTerms, t);
+                const T c = t[0];
+                if (!(c > tneg_inf<T>())) continue;
+                const T lt = log_term<T, K>(c, t + 2, t + 8, zm);
+                if (lt > mx) { acc = acc * texp_sum(mx - lt) + T(1); mx = lt; }   // online log-sum-exp
+                else acc += texp_sum(lt - mx);
+                if (lt >= cand_min) {
+                    if (n_cand < kLikCand) s_cand[n_cand * blockDim.x + threadIdx.x] = k;
+                    ++n_cand;
+                }
             }
         }
     }
     T ell = bpc;
-    if (m < M && mx > tneg_inf<T>()) {
+    if (m < M && fixed_shift) {
+        ell = s0 + tlog(acc + texp(bpc - s0));   // (sum_j exp(lt_j)) (+) bpc
+    } else if (m < M && mx > tneg_inf<T>()) {
         // (sum_j exp(lt_j)) (+) bpc, evaluated around the larger of the two
         T big = mx > bpc ? mx : bpc;
         ell = big + tlog(acc * texp(mx - big) + texp(bpc - big));
