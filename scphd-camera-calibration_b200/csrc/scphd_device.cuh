@@ -520,12 +520,12 @@ __device__ inline void kalman_prep(T w, T pdbar, const T* P, const Model& m, T* 
         Kg[q] = acc;
         dst[kPrepK + q] = acc;
     }
-    // Joseph entry e = (ea, eb)
+    // Joseph entry e = (ea, eb), ea >= eb
 #pragma unroll
-    for (int e = 0; e < 21; ++e) {
-        int ea = 0;
-        while ((ea + 1) * (ea + 2) / 2 <= e) ++ea;
-        const int eb = e - ea * (ea + 1) / 2;
+    for (int ea = 0; ea < 6; ++ea)
+#pragma unroll
+    for (int eb = 0; eb <= ea; ++eb) {
+        const int e = tri(ea, eb);
         T sv = P[e];
 #pragma unroll
         for (int k = 0; k < K; ++k) {

@@ -171,23 +171,20 @@ __global__ void k_predict_parents(__grid_constant__ const Params prm, double* ex
 template <typename T, typename V, int W>
 __device__ __forceinline__ void ltz_line(const T* line, const T z[6], T y[6]) {
     const V* v = reinterpret_cast<const V*>(line);
-#pragma unroll
-    for (int a = 0; a < 6; ++a) y[a] = 0;
+    T e[28];
 #pragma unroll
     for (int i = 0; i < 28 / W; ++i) {
         const V q = v[i];
-        const T* e = reinterpret_cast<const T*>(&q);
+        const T* x = reinterpret_cast<const T*>(&q);
 #pragma unroll
-        for (int h = 0; h < W; ++h) {
-            const int k = i * W + h;
-            if (k < 21) {
-                int a = 0;
-                while ((a + 1) * (a + 2) / 2 <= k) ++a;
-                y[a] += e[h] * z[k - a * (a + 1) / 2];
-            } else if (k < 27) {
-                y[k - 21] += e[h];
-            }
-        }
+        for (int h = 0; h < W; ++h) e[i * W + h] = x[h];
+    }
+#pragma unroll
+    for (int a = 0; a < 6; ++a) {
+        T s = T(0);
+#pragma unroll
+        for (int c = 0; c <= a; ++c) s += e[tri(a, c)] * z[c];
+        y[a] = s + e[21 + a];
     }
 }
 __device__ __forceinline__ void ltz_plus_mean(const float* line, const float z[6], float y[6]) {
@@ -302,7 +299,9 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
         // nearly always of one kind and the sample loop does not diverge)
         int refg[2] = {0, 0};
         T Wg[2] = {T(0), T(0)};
-        for (int g = 0; g < nG; ++g) {
+#pragma unroll
+        for (int g = 0; g < 2; ++g) {   // static indices: refg and Wg stay in registers
+            if (g >= nG) break;
             const size_t erow = (size_t)row * prm.Gcap + j0 + g;
             const T* ent = b.map[cur] + erow * kRow;
             const int ref = b.map_ref[cur][erow];
@@ -395,7 +394,11 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
                         const T v = __shfl_sync(0xffffffffu, y[a2], lane & 16);
                         shift[a2] = isfinite(v) ? v : T(0);
                     }
-                    if (hl < 6 && gvalid) shift_g[hl] = shift[hl];
+                    if (gvalid) {   // static indices: the shift stays in registers
+#pragma unroll
+                        for (int a2 = 0; a2 < 6; ++a2)
+                            if (hl == a2) shift_g[a2] = shift[a2];
+                    }
                 }
                 if (stage && gvalid && s < P4) {
                     if (raw) {
