@@ -273,6 +273,54 @@ def test_fp32_frames_track_oracle(pkg, orc):
             break   # ancestries diverge from here on; the comparison ends
 
 
+def _state(f):
+    """A filter's whole state as set_state takes it."""
+    st, lw = f.particles()
+    sizes = f.map_sizes()
+    ws, cl, om = [], [], []
+    for p in range(f.n_parents):
+        if sizes[p]:
+            ws.append(f.map_weights(p))
+            x, o = f.map_clouds(p)
+            cl.append(x)
+            om.append(o)
+    P = int(f.config.particles_per_feature)
+    cat = lambda xs, shp: np.concatenate(xs) if xs else np.zeros(shp)
+    return st, lw, sizes, cat(ws, (0,)), cat(cl, (0, 6, P)), cat(om, (0, P))
+
+
+@pytest.mark.parametrize("clutter", [5.0, 1e-30])
+def test_fp32_one_step_normalisers(pkg, clutter):
+    """One FP64 state loaded into a fresh FP64 and a fresh FP32 filter; the next
+    predict + update's normalisers agree to FP32 accuracy.  With clutter 5 the FP32
+    normaliser sums around the parent's largest log-constant; with clutter 1e-30 per
+    frame log(M w0 + kappa) is about -85, more than 60 below the Gaussians'
+    log-constants, and it takes its online log-sum-exp.  (Run on, the two modes part
+    at a prune decision on a threshold there, so the comparison is one step.)"""
+    _need_gpu()
+    sc = pkg.scene.make_scene(n_landmarks=25, n_frames=5, clutter_rate=clutter, seed=pkg.scene.scene_seed(0, 12))
+    cfg = pkg.scene.filter_config(n_parents=64, max_gaussians=160, max_meas=96, clutter_rate=clutter,
+                                  precision=pkg.SCPHD_FP64, calib=sc.calib, seed=12, particles_per_feature=100)
+    src = pkg.SCPHDCameraCalibration(cfg)
+    for k in range(3):
+        z = sc.frames[k]
+        src.step(pkg.scene.DT, z[:, 0], z[:, 1], fixed_camera=sc.fixed[k], d=z[:, 2])
+    state = _state(src)
+    out = []
+    for prec in (pkg.SCPHD_FP64, pkg.SCPHD_FP32):
+        c = cfg.copy()
+        c.precision = prec
+        f = pkg.SCPHDCameraCalibration(c)
+        f.set_state(*state)
+        z = sc.frames[3]
+        f.predict(pkg.scene.DT)
+        f.update(z[:, 0], z[:, 1], fixed_camera=sc.fixed[3], d=z[:, 2])
+        out.append(f.normalizers(z.shape[0])[0])
+    e64, e32 = out
+    rel = np.abs(e32 - e64) / np.maximum(1.0, np.abs(e64))
+    assert np.median(rel) < 1e-5 and np.quantile(rel, 0.99) < 1e-3, (np.median(rel), np.quantile(rel, 0.99))
+
+
 @pytest.mark.parametrize("prec", [1, 0])
 def test_map_capacity_keeps_largest_weights(pkg, orc, prec):
     """max_gaussians binds: the new map holds the max_gaussians largest weights of
