@@ -721,9 +721,10 @@ __global__ void __launch_bounds__(1024)
 }
 
 // ---------------------------------------------------------------- (d) merge
-// Posterior components of one parent (detections and births) by survivor rank r:
-// the mean from the fitted row, Kalman gain and measurement; the covariance is
-// Gaussian j's posterior (prep rows) or the birth covariance.
+// Posterior components of one parent (detections and births) by survivor rank r: the
+// mean, from the fitted row, the Kalman gain and the measurement (a birth's from the
+// birth template); bcov holds the birth covariance, the detections' covariances are
+// their Gaussians' posteriors in the prep rows.
 template <typename T, int K> struct KalmanSource {
     const T* fit;   // parent's fitted rows
     const T* prep;  // parent's prep rows
