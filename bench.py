@@ -640,8 +640,8 @@ def run_precision(args, pkg):
     compared: parent log-likelihoods, per-measurement log normalisers, fitted
     mixtures (rows correspond one to one) and merged mixtures (rows paired by
     nearest mean).
-    (2) Trajectories at full size: FP64 and FP32 runs on the same seed and an FP64
-    run on a second seed; once resampling differs the runs are different Monte-Carlo
+    (2) Trajectories at full size: FP64 and FP32 runs on each of --precision-seeds
+    filter seeds (the scene is the same); once resampling differs the runs are different Monte-Carlo
     realisations, so the FP32-FP64 differences of OSPA and calibration error are
     set against the FP64 seed-to-seed spread."""
     import torch
@@ -701,8 +701,11 @@ def run_precision(args, pkg):
         f.close()
     # ---- (2) trajectories at full size
     traj = {}
-    for name, prec, seed_off in (("fp64", pkg.SCPHD_FP64, 0), ("fp32", pkg.SCPHD_FP32, 0),
-                                 ("fp64_seed2", pkg.SCPHD_FP64, 1)):
+    n_seeds = max(2, args.precision_seeds)
+    runs = []
+    for seed_off in range(n_seeds):
+        runs += [("fp64_s%d" % seed_off, pkg.SCPHD_FP64, seed_off), ("fp32_s%d" % seed_off, pkg.SCPHD_FP32, seed_off)]
+    for name, prec, seed_off in runs:
         sc, cfg = pkg.scene.workload("precision_c3", precision=prec, n_frames=n_frames)
         cfg.seed = int(cfg.seed) + 7919 * seed_off
         if args.parents:
@@ -718,11 +721,14 @@ def run_precision(args, pkg):
             f.update_device(z[0].data_ptr(), z[1].data_ptr(), z[2].data_ptr(), z.shape[1], sc.fixed[k])
             f.synchronize()
             t_dev += time.perf_counter() - t0
-            st, lw = f.particles()
-            m = pkg.evaluate.frame_metrics(st, lw, f.map_weights, lambda p: f.map_clouds(p)[0], sc, k)
-            pose = pkg.evaluate.expected_pose(st, lw)
-            rows.append([m["ospa"], m["calib_position_m"], m["calib_angle_rad"], m["n_features"],
-                         m["cardinality"], *pose[[0, 1, 2, 6, 7, 8]]])
+            if k >= n_frames // 2 or k == n_frames - 1:   # the summaries use the second half
+                st, lw = f.particles()
+                m = pkg.evaluate.frame_metrics(st, lw, f.map_weights, lambda p: f.map_clouds(p)[0], sc, k)
+                pose = pkg.evaluate.expected_pose(st, lw)
+                rows.append([m["ospa"], m["calib_position_m"], m["calib_angle_rad"], m["n_features"],
+                             m["cardinality"], *pose[[0, 1, 2, 6, 7, 8]]])
+            else:
+                rows.append([np.nan] * 11)
             t0 = time.perf_counter()
             f.resample()
             f.synchronize()
@@ -734,7 +740,7 @@ def run_precision(args, pkg):
         del dz
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
-    a, b, c = traj["fp64"], traj["fp32"], traj["fp64_seed2"]
+    a, b = traj["fp64_s0"], traj["fp32_s0"]
     aligned = 0
     for k in range(min(len(a["idx"]), len(b["idx"]))):
         if not np.array_equal(a["idx"][k], b["idx"][k]):
@@ -742,14 +748,20 @@ def run_precision(args, pkg):
         aligned = k + 1
     tail = slice(n_frames // 2, None)
     mean = lambda r, j: float(r["rows"][tail, j].mean())
-    summ = {"frames": n_frames, "one_step": local, "resampling_identical_frames": aligned}
+    summ = {"frames": n_frames, "seeds": n_seeds, "one_step": local, "resampling_identical_frames": aligned}
     for j, nm in ((0, "ospa"), (1, "calib_position_m"), (2, "calib_angle_rad"), (3, "n_features")):
-        summ[nm] = {"fp64": mean(a, j), "fp32": mean(b, j), "fp64_seed2": mean(c, j),
-                    "fp32_minus_fp64": mean(b, j) - mean(a, j), "seed_spread_fp64": mean(c, j) - mean(a, j)}
-        summ[nm + "_final"] = {"fp64": float(a["rows"][-1, j]), "fp32": float(b["rows"][-1, j]),
-                               "fp64_seed2": float(c["rows"][-1, j])}
+        v64 = np.array([mean(traj["fp64_s%d" % i], j) for i in range(n_seeds)])
+        v32 = np.array([mean(traj["fp32_s%d" % i], j) for i in range(n_seeds)])
+        diff = float(v32.mean() - v64.mean())
+        se = float(np.sqrt(v64.var(ddof=1) / n_seeds + v32.var(ddof=1) / n_seeds))
+        summ[nm] = {"fp64": v64.tolist(), "fp32": v32.tolist(), "fp64_mean": float(v64.mean()),
+                    "fp32_mean": float(v32.mean()), "fp32_minus_fp64": diff, "diff_standard_error": se,
+                    "diff_rel": diff / float(v64.mean()), "diff_rel_95": (abs(diff) + 1.96 * se) / float(v64.mean()),
+                    "seed_sd_fp64": float(v64.std(ddof=1))}
+        summ[nm + "_final"] = {k2: float(v["rows"][-1, j]) for k2, v in traj.items()}
     summ["seconds"] = {k2: v["seconds"] for k2, v in traj.items()}
-    summ["note"] = "trajectory figures are means over the second half of the frames"
+    summ["note"] = ("trajectory figures are means over the second half of the frames, per seed; "
+                    "diff_rel_95 = (|mean FP32 - mean FP64| + 1.96 standard errors) / mean FP64")
     if args.precision_dump:
         np.savez_compressed(args.precision_dump, **{k2: v["rows"] for k2, v in traj.items()})
     return summ
@@ -772,6 +784,7 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="serving window of serving_c4")
     ap.add_argument("--precision-frames", type=int, default=300, help="frames of the precision_c3 study")
     ap.add_argument("--precision-dump", default="", help="npz of the per-frame trajectories")
+    ap.add_argument("--precision-seeds", type=int, default=3, help="filter seeds per precision in the trajectories")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
