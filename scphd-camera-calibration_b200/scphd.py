@@ -23,6 +23,14 @@ SCPHD_FP64 = 1
 SCPHD_MIX_FITTED = 0
 SCPHD_MIX_MERGED = 1
 
+# names of the 16 counters of scphd_get_counters, in the order include/scphd.h gives them
+COUNTER_NAMES = (
+    "map_truncations", "scratch_overflows", "frames_updated", "resamplings",
+    "units_last_update", "survivors_last_update", "units_total", "survivors_total",
+    "clouds_read", "clouds_written", "gaussians_fitted", "merged_rows",
+    "mahalanobis_evaluations", "max_survivors_per_parent", "unit_weight_fits", "reserved",
+)
+
 _STATUS = {0: "OK", 1: "INVALID", 2: "CUDA", 3: "CAPACITY", 4: "NAN", 5: "NO_DEVICE"}
 
 
@@ -444,6 +452,10 @@ class SCPHDCameraCalibration:
         c = np.zeros(16, np.int64)
         _check(self._lib.scphd_get_counters(self._h, c.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
         return c
+
+    def counters_by_name(self) -> dict:
+        """scphd_get_counters as {name: value} (names: COUNTER_NAMES)."""
+        return dict(zip(COUNTER_NAMES, (int(v) for v in self.counters())))
 
     @property
     def stream_handle(self) -> int:

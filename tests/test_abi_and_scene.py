@@ -98,3 +98,23 @@ def test_device_bytes_and_wave_plan(pkg):
     assert all(sum(sizes[i] for i in w) <= 10 for w in waves)
     with pytest.raises(ValueError):
         pkg.scene.plan_waves([11], 10)
+
+
+def test_counter_names_follow_the_header(pkg):
+    """COUNTER_NAMES lists scphd_get_counters' entries in the order the header documents."""
+    with open(os.path.join(ROOT, "include", "scphd.h")) as fh:
+        text = " ".join(fh.read().split())
+    doc = text[text.index("Counters since create:"):text.index("scphd_status scphd_get_counters")]
+    parts = re.split(r"\[(\d+)\]", doc)
+    entries = {int(parts[i]): parts[i + 1] for i in range(1, len(parts) - 1, 2)}
+    assert sorted(entries) == list(range(16))
+    keyword = {"map_truncations": "truncation", "scratch_overflows": "overflow", "frames_updated": "frames updated",
+               "resamplings": "resampling", "units_last_update": "units of the last",
+               "survivors_last_update": "survivors of the last", "units_total": "units since",
+               "survivors_total": "survivors since", "clouds_read": "read", "clouds_written": "written",
+               "gaussians_fitted": "fitted", "merged_rows": "merged", "mahalanobis_evaluations": "Mahalanobis",
+               "max_survivors_per_parent": "largest survivor", "unit_weight_fits": "unit sample",
+               "reserved": "reserved"}
+    assert len(pkg.COUNTER_NAMES) == 16 and set(pkg.COUNTER_NAMES) == set(keyword)
+    for k, name in enumerate(pkg.COUNTER_NAMES):
+        assert keyword[name] in entries[k], (k, name, entries[k])
