@@ -113,8 +113,10 @@ template <> struct Pair<float> {
         float ua = __fmaf_rn((float)wa, 0x1p-32f, 0x1p-33f);
         float ub = __fmaf_rn((float)wb, 0x1p-32f, 0x1p-33f);
         ua = fminf(ua, 0.99999994f);
-        const float r2 = -2.0f * __logf(ua);   // > 0: ua < 1
-        float r = r2 * rsqrtf(r2);
+        // the approximate log (absolute error up to about 1e-7 near 1) of the largest u_a
+        // below 1 can come out as 0 or above: r is 0 there instead of NaN
+        const float r2 = -2.0f * __logf(ua);
+        const float r = r2 > 0.0f ? r2 * rsqrtf(r2) : 0.0f;
         float th = 6.283185307179586f * (ub - 0.5f);
         float s, c;
         __sincosf(th, &s, &c);
