@@ -132,73 +132,94 @@ def replica_seed_index(rank: int) -> int:
     return rank
 
 
-def cpu_oracle_rate(pkg, workload: str, sample_parents: int, prefill: int, frames: int, threads: int):
-    """Units/s of the FP64 oracle (the CPU restatement of the reference) on a
-    bounded sample of the workload: the same scene with `sample_parents` parents."""
+CPU_SAMPLE_PARENTS = 32   # parents of the workload's scene in the timed CPU sample
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def _oracle_step(o, sc, k, DT):
+    z = sc.frames[k]
+    g = int(o.map_sizes().sum())
+    t0 = time.perf_counter()
+    o.predict(DT)
+    o.update(z[:, 0], z[:, 1], sc.fixed[k], d=z[:, 2])
+    o.resample()
+    return g * z.shape[0], time.perf_counter() - t0
+
+
+def cpu_sample(pkg, workload: str, sample_parents: int, prefill: int, frames: int, threads_list):
+    """Units/s of the FP64 oracle (the CPU restatement of the reference's filter step,
+    with the same map capacity as the device) on a bounded sample of the workload:
+    the workload's scene and configuration with `sample_parents` parents.  `prefill`
+    untimed frames (all threads) populate the maps; their end state is copied into a
+    fresh oracle per thread count, and the same `frames` frames are timed from it, so
+    every thread count does identical work.  Units/s is additive over parents."""
     sys.path.insert(0, ROOT)
     from oracle import oracle as orc
     orc.build()
-    used = orc.set_threads(threads)
+    all_threads = os.cpu_count() or 1
     sc, cfg = pkg.scene.workload(workload, precision=pkg.SCPHD_FP64, n_frames=prefill + frames)
-    cfg.n_parents = sample_parents
+    cfg.n_parents = min(int(cfg.n_parents), sample_parents)
+    orc.set_threads(all_threads)
     o = orc.Oracle(cfg)
-    units, t = 0, 0.0
-    for k in range(prefill + frames):
-        z = sc.frames[k]
-        g = int(o.map_sizes().sum())
-        t0 = time.perf_counter()
-        o.predict(pkg.scene.DT)
-        o.update(z[:, 0], z[:, 1], sc.fixed[k], d=z[:, 2])
-        o.resample()
-        dt = time.perf_counter() - t0
-        if k >= prefill:
-            units += g * z.shape[0]
-            t += dt
-    return units / t, used, units, t
+    for k in range(prefill):
+        _oracle_step(o, sc, k, pkg.scene.DT)
+    snap = o.state()
+    out = {}
+    for th in threads_list:
+        used = orc.set_threads(th)
+        oc = orc.Oracle(cfg)
+        oc.load(snap)
+        units, secs = 0, []
+        for k in range(prefill, prefill + frames):
+            u, dt = _oracle_step(oc, sc, k, pkg.scene.DT)
+            units += u
+            secs.append(dt)
+        out[th] = {"value": units / sum(secs), "threads": used, "units": units, "seconds": sum(secs),
+                   "ms_per_frame": 1e3 * sum(secs) / len(secs), "truncations": oc.truncations()}
+    orc.set_threads(all_threads)
+    return out, int(cfg.n_parents)
 
 
 def run_reference(args):
-    """--impl reference: the reference's CPU path (the oracle port of it) on the host cores."""
+    """--impl reference: the reference's filter step on the host cores -- the oracle,
+    the project's C++ restatement of it (the reference's own program cannot be built
+    here: it needs libconfig, matio, the CUDA SDK helpers and compute_20) -- on the
+    same bounded sample of the workload as the b200 arm's cpu_baseline leg, all host
+    threads.  Config 0 (plain_c0) is host-sized and runs at full size from frame 0."""
     world, rank, _ = dist_env()
     if rank != 0:
         return
     pkg = load_package()
     threads = os.cpu_count() or 1
-    sample = min(4096, max(64, 2 * threads))
-    sys.path.insert(0, ROOT)
-    from oracle import oracle as orc
-    orc.build()
-    used = orc.set_threads(threads)
-    sc, cfg = pkg.scene.workload(args.workload, precision=pkg.SCPHD_FP64,
-                                 n_frames=args.prefill + args.warmup + args.steps)
-    cfg.n_parents = sample
-    o = orc.Oracle(cfg)
-    k = 0
-    times, units = [], []
-    for phase, n in (("prefill", args.prefill), ("warmup", args.warmup), ("timed", args.steps)):
-        for _ in range(n):
-            z = sc.frames[k]
-            g = int(o.map_sizes().sum())
-            t0 = time.perf_counter()
-            o.predict(pkg.scene.DT)
-            o.update(z[:, 0], z[:, 1], sc.fixed[k], d=z[:, 2])
-            o.resample()
-            dt = time.perf_counter() - t0
-            if phase == "timed":
-                times.append(dt)
-                units.append(g * z.shape[0])
-            k += 1
-    value = sum(units) / sum(times)
+    full = args.workload == "plain_c0"
+    prefill = (0 if full else args.cpu_prefill) + args.warmup   # warm-up frames are untimed
+    sample = 1 << 30 if full else CPU_SAMPLE_PARENTS
+    res, n_used = cpu_sample(pkg, args.workload, sample, prefill, args.steps, [threads])
+    r = res[threads]
+    n_full = int(pkg.scene.WORKLOADS[args.workload]["n_parents"])
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / len(times),
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_frame"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "n_parents": sample, "n_parents_full": 4096,
-                   "note": "parent sample of the workload; units/s is per-parent-additive"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": "port",
-                         "sample": f"{sample} of 4096 parents of {args.workload}, {args.prefill} untimed frames "
-                                   f"to populate the maps, then {args.warmup}+{args.steps} frames"},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": {"workload": args.workload, "n_parents": n_used, "n_parents_full": n_full,
+                   "note": "parent sample of the workload; units/s is additive over parents"},
+        "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["threads"], "kind": "port",
+                         "cpu_model": cpu_model(), "nproc": threads,
+                         "sample": f"{n_used} of {n_full} parents of {args.workload}, {prefill} untimed frames "
+                                   f"(map population and warm-up), then {args.steps} timed frames "
+                                   f"({r['seconds']:.1f} s)"},
+        "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
@@ -252,6 +273,7 @@ def run_b200(args):
     clocks = ClockSampler(local)
     clocks.start()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(K + 1)]
+    timed_meas = [int(sc.frames[k + i].shape[0]) for i in range(K)]
     ev[0].record(stream)
     for i in range(K):
         dstep()
@@ -342,21 +364,32 @@ def run_b200(args):
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        sample = min(4096, max(32, threads))
-        rate, used, cu, ct = cpu_oracle_rate(pkg, args.workload, sample, args.cpu_prefill, args.cpu_frames, threads)
-        cpu = {"value": rate, "unit": UNIT, "cores": used, "kind": "port",
-               "sample": f"{sample} of {cfg.n_parents} parents of {args.workload}, {args.cpu_prefill} untimed "
-                         f"frames to populate the maps, {args.cpu_frames} timed frames ({ct:.1f} s)"}
+        res, n_used = cpu_sample(pkg, args.workload, CPU_SAMPLE_PARENTS, args.cpu_prefill, args.cpu_frames,
+                                 [threads, 1])
+        ra, r1 = res[threads], res[1]
+        cpu = {"value": ra["value"], "unit": UNIT, "cores": ra["threads"], "kind": "port",
+               "threads_all": {"threads": ra["threads"], "value": ra["value"], "ms_per_frame": ra["ms_per_frame"]},
+               "threads_1": {"threads": 1, "value": r1["value"], "ms_per_frame": r1["ms_per_frame"]},
+               "cpu_model": cpu_model(), "nproc": threads,
+               "sample": f"{n_used} of {cfg.n_parents} parents of {args.workload}, {args.cpu_prefill} untimed "
+                         f"frames to populate the maps, then the same {args.cpu_frames} frames timed at "
+                         f"{ra['threads']} threads ({ra['seconds']:.1f} s) and at 1 thread ({r1['seconds']:.1f} s)"}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_all / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": args.precision, "data": "synthetic",
-        "config": {"workload": args.workload, "n_parents": int(cfg.n_parents), "landmarks": 200,
-                   "clutter_rate": 50.0, "max_gaussians": int(cfg.max_gaussians),
+        "config": {"workload": args.workload, "n_parents": int(cfg.n_parents),
+                   "landmarks": int(pkg.scene.WORKLOADS[args.workload]["n_landmarks"]),
+                   "clutter_rate": float(pkg.scene.WORKLOADS[args.workload]["clutter"]),
+                   "max_gaussians": int(cfg.max_gaussians),
                    "particles_per_feature": P, "meas_dim": int(cfg.meas_dim), "prefill_frames": args.prefill,
                    "mean_gaussians_per_parent": fitted / max(1, K) / cfg.n_parents,
-                   "mean_measurements": units / max(1, fitted / K * 1.0) / K if fitted else None,
+                   "mean_measurements": float(np.mean(timed_meas)),
+                   "measurements_note": "the landmark box (10 x 10 x 10 m, 2-12 m ahead) extends beyond the "
+                                        "640x480 field of view, so fewer landmarks are seen than the ~240 "
+                                        "measurements per frame the config names (200 pD + 50 clutter); "
+                                        "units are G x M, so this understates throughput",
                    "l2": "no flush: the resident map/cloud state is larger than L2",
                    "parallelism": f"replicas{world}", "launch_shapes": shapes},
         "frame_ms": {"p50": float(np.percentile(frame_ms, 50)), "p99": float(np.percentile(frame_ms, 99)),

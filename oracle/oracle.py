@@ -24,10 +24,12 @@ VP = ctypes.c_void_p
 STAGE_PRIOR, STAGE_CAM, STAGE_FEAT, STAGE_SAMPLE, STAGE_RESAMPLE = 1, 2, 3, 4, 5
 
 
-def build(ref_dir: str = "/root/reference") -> None:
-    """Build liboracle.so, and _ref/libscphd_ref.so when the reference tree exists."""
+def build(ref_dir: str | None = None) -> None:
+    """Build liboracle.so, and _ref/libscphd_ref.so when a reference tree is given
+    (argument, or the REF_DIR environment variable) and holds the sources."""
     subprocess.run(["make", "-s", "liboracle.so"], cwd=HERE, check=True)
-    if os.path.isdir(os.path.join(ref_dir, "src")):
+    ref_dir = ref_dir or os.environ.get("REF_DIR")
+    if ref_dir and os.path.isdir(os.path.join(ref_dir, "src")):
         subprocess.run(["make", "-s", "ref", f"REF_DIR={ref_dir}"], cwd=HERE, check=True)
 
 
@@ -61,6 +63,7 @@ def lib():
             "orc_update": (None, [VP, P(D), P(D), P(D), I32, I32]),
             "orc_resample": (I32, [VP]),
             "orc_frame": (I32, [VP]),
+            "orc_set_frame": (None, [VP, I32]),
             "orc_get_particles": (None, [VP, P(D), P(D)]),
             "orc_map_size": (I32, [VP, I32]),
             "orc_get_map": (None, [VP, I32, P(D), P(D), P(D)]),
@@ -84,6 +87,8 @@ def lib():
             "orc_measure": (None, [VP, P(D), P(D), P(D)]),
             "orc_invert": (None, [VP, P(D), P(D), P(D)]),
             "orc_detect": (None, [VP, P(D), P(D), P(D)]),
+            "orc_cap_keep": (None, [P(D), I32, I32, P(U8)]),
+            "orc_truncations": (ctypes.c_int64, [VP]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(L, name)
@@ -127,6 +132,22 @@ class Oracle:
     @property
     def frame(self) -> int:
         return int(lib().orc_frame(self._h))
+
+    def set_frame(self, frame: int) -> None:
+        lib().orc_set_frame(self._h, int(frame))
+
+    def state(self):
+        """The whole state as set_state takes it (with the frame counter)."""
+        st, lw = self.particles()
+        sizes = self.map_sizes()
+        parts = [self.map(p) for p in range(self.N)]
+        cat = lambda i, shp: np.concatenate([q[i] for q in parts]) if sizes.sum() else np.zeros(shp)
+        return (st, lw, sizes, cat(0, (0,)), cat(1, (0, 6, self.P)), cat(2, (0, self.P))), self.frame
+
+    def load(self, state_and_frame) -> None:
+        state, frame = state_and_frame
+        self.set_state(*state)
+        self.set_frame(frame)
 
     def particles(self):
         st = np.zeros((self.N, 12))
@@ -175,6 +196,10 @@ class Oracle:
         s = np.zeros(self.N, np.int32)
         lib().orc_get_survivors(self._h, _i(s))
         return s
+
+    def truncations(self) -> int:
+        """Maps cut at max_gaussians since create."""
+        return int(lib().orc_truncations(self._h))
 
     def resample_indices(self):
         idx = np.zeros(self.N, np.int32)
@@ -226,6 +251,14 @@ def merge(comps, flags, min_sep):
     mem = np.zeros(max(n, 1), np.int32)
     lib().orc_merge(_d(comps), fl.ctypes.data_as(P(U8)), n, float(min_sep), _d(out), ctypes.byref(nout), _i(mem))
     return out[: nout.value], mem[:n]
+
+
+def cap_keep(w, cap):
+    """Entries kept when a map with entry weights w is cut to cap entries."""
+    w = _f64(w)
+    keep = np.zeros(w.size, np.uint8)
+    lib().orc_cap_keep(_d(w), int(w.size), int(cap), keep.ctypes.data_as(P(U8)))
+    return keep.astype(bool)
 
 
 def systematic(w, u01):

@@ -31,7 +31,9 @@
 //   * maps are keyed per parent explicitly, so the reduce_by_key defects on empty
 //     maps and M == 1 (:1750-1756, :2562-2585) do not arise;
 //   * meas_dim 3 generalises H = [I_2 0] to [I_3 0] and births take the measured d;
-//   * a stereo baseline multiplies d and vd (baseline 1 is the reference).
+//   * a stereo baseline multiplies d and vd (baseline 1 is the reference);
+//   * a parent's map is capped at max_gaussians entries, keeping the largest
+//     weights (the reference's maps are unbounded).
 #include "scphd.h"
 
 #include <algorithm>
@@ -263,6 +265,16 @@ void merge_map(const std::vector<G6>& comps, std::vector<uint8_t>& flags, double
     }
 }
 
+// Entries kept when a map of weights w is cut to cap entries: the cap largest
+// weights, equal weights in entry order (a stable sort by decreasing weight).
+void cap_keep(const std::vector<double>& w, int cap, std::vector<char>& keep) {
+    std::vector<int> order(w.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return w[a] > w[b]; });
+    keep.assign(w.size(), 0);
+    for (int i = 0; i < cap && i < (int)w.size(); ++i) keep[order[i]] = 1;
+}
+
 // systematic resampling as written, src/scphdcameracalibration.cu:2660-2702
 void systematic(const std::vector<double>& w, double r0, std::vector<int>& idx) {
     const int n = (int)w.size();
@@ -297,6 +309,7 @@ struct Oracle {
     int N, P, K;
     int frame = 0;
     int weight_mode = 0;   // 0 log domain, 1 linear as written
+    long long truncations = 0;   // maps cut at max_gaussians since create
     std::vector<Ext> ext;
     std::vector<double> lw;          // log weights (mode 0) or linear weights (mode 1)
     std::vector<std::vector<Cloud>> maps;
@@ -495,6 +508,29 @@ struct Oracle {
         if (!is_pos_def6_strict(out.cov)) out.w = safe_log(0);   // kernels.cu:597-598
     }
 
+    // Map capacity.  The reference keeps every merged component and every retained
+    // non-detection cloud (compaction src/scphdcameracalibration.cu:1923-1942 copies
+    // all of them); this implementation bounds a parent's map at max_gaussians
+    // entries.  When the new map (merged components in merge order, then the retained
+    // non-detection clouds in Gaussian order) holds more, the max_gaussians entries of
+    // largest weight are kept, equal weights in entry order, and the kept entries
+    // keep their order.  max_gaussians <= 0 means no cap.
+    void cap_map(std::vector<Cloud>& out) {
+        const int cap = cfg.max_gaussians;
+        if (cap <= 0 || (int)out.size() <= cap) return;
+        std::vector<double> w(out.size());
+        for (size_t i = 0; i < out.size(); ++i) w[i] = out[i].W;
+        std::vector<char> keep;
+        cap_keep(w, cap, keep);
+        std::vector<Cloud> kept;
+        kept.reserve(cap);
+        for (size_t i = 0; i < out.size(); ++i)
+            if (keep[i]) kept.push_back(std::move(out[i]));
+        out.swap(kept);
+#pragma omp atomic
+        ++truncations;
+    }
+
     static double lse(double a, double b) {   // log_sum_exp functor, .cu:506-517
         if (a > b) return a + safe_log(1 + std::exp(b - a));
         return b + safe_log(1 + std::exp(a - b));
@@ -656,6 +692,7 @@ struct Oracle {
                 c.x.swap(X6);
                 out.push_back(std::move(c));
             }
+            cap_map(out);
             mp.swap(out);
         }
         if (!fixed) {   // parent weights, .cu:1813-1876
@@ -745,6 +782,9 @@ void orc_update(void* h, const double* u, const double* v, const double* d, int 
 }
 int orc_resample(void* h) { return static_cast<Oracle*>(h)->resample(); }
 int orc_frame(void* h) { return static_cast<Oracle*>(h)->frame; }
+// the frame counter keys the random streams: a state copied into a fresh oracle with
+// the same counter replays the same work
+void orc_set_frame(void* h, int frame) { static_cast<Oracle*>(h)->frame = frame; }
 
 void orc_get_particles(void* h, double* states, double* logw) {
     Oracle* o = static_cast<Oracle*>(h);
@@ -845,6 +885,14 @@ double orc_mahal6(const double* a28, const double* b28) {
 int orc_is_pos_def(const double* cov36) { return is_pos_def6(cov36); }
 double orc_wrap_angle(double a) { return wrap_angle(a); }
 uint32_t orc_tie_key(uint32_t r) { return tie_key(r); }
+// the map-capacity cut on a list of entry weights: keep[i] = 1 for kept entries
+void orc_cap_keep(const double* w, int n, int cap, uint8_t* keep) {
+    std::vector<double> ww(w, w + n);
+    std::vector<char> k;
+    cap_keep(ww, cap, k);
+    for (int i = 0; i < n; ++i) keep[i] = (uint8_t)k[i];
+}
+long long orc_truncations(void* h) { return static_cast<Oracle*>(h)->truncations; }
 
 // world -> disparity of one point with extrinsic e (12), using the filter's model
 void orc_measure(void* h, const double* X, const double* e12, double* y) {

@@ -873,6 +873,8 @@ scphd_status scphd_merge_components(const double* comps, const uint8_t* flags, i
     if (n < 0 || (n > 0 && (!comps || !flags || !merged || !n_out))) return fail(SCPHD_ERR_INVALID, "bad arguments");
     if (n > 2048) return fail(SCPHD_ERR_CAPACITY, "at most 2048 components");
     if (!(min_separation > 0)) return fail(SCPHD_ERR_INVALID, "min_separation must be > 0");
+    if (precision != SCPHD_FP32 && precision != SCPHD_FP64)
+        return fail(SCPHD_ERR_INVALID, "precision must be SCPHD_FP32 or SCPHD_FP64");
     if (n_out) *n_out = 0;
     if (n == 0) return SCPHD_OK;
     int dev = 0;
@@ -901,20 +903,27 @@ scphd_status scphd_merge_components(const double* comps, const uint8_t* flags, i
                 st = fail(SCPHD_ERR_CUDA, "allocation for merge_components failed");
                 break;
             }
-            cudaMemcpy(d_rows, rows.data(), sizeof(T) * rows.size(), cudaMemcpyHostToDevice);
-            cudaMemcpy(d_flags, flags, n, cudaMemcpyHostToDevice);
-            cudaMemset(d_mem, 0xff, sizeof(int) * n);
-            allow_dynamic_smem((const void*)k_merge_list<T>);
+            // every runtime call is checked: a failed copy or launch must not leave the
+            // host reading uninitialised device memory as a result
+            auto check = [&](cudaError_t e, const char* what) {
+                if (e != cudaSuccess && st == SCPHD_OK)
+                    st = fail(SCPHD_ERR_CUDA, std::string("merge_components ") + what + ": " + cudaGetErrorString(e));
+                return st == SCPHD_OK;
+            };
+            if (!check(cudaMemcpy(d_rows, rows.data(), sizeof(T) * rows.size(), cudaMemcpyHostToDevice), "copy in") ||
+                !check(cudaMemcpy(d_flags, flags, n, cudaMemcpyHostToDevice), "copy flags") ||
+                !check(cudaMemset(d_mem, 0xff, sizeof(int) * n), "memset") ||
+                !check(cudaMemset(d_n, 0, sizeof(int)), "memset") ||
+                !check(allow_dynamic_smem((const void*)k_merge_list<T>), "shared memory attribute"))
+                break;
             k_merge_list<T><<<1, 128, smem>>>(d_rows, d_flags, n, (T)min_separation, d_sparse, d_out, d_n, d_mem);
             g_launches.fetch_add(1, std::memory_order_relaxed);
-            cudaError_t e = cudaDeviceSynchronize();
-            if (e != cudaSuccess) {
-                st = fail(SCPHD_ERR_CUDA, std::string("k_merge_list: ") + cudaGetErrorString(e));
+            if (!check(cudaGetLastError(), "launch") || !check(cudaDeviceSynchronize(), "k_merge_list")) break;
+            if (!check(cudaMemcpy(&nout, d_n, sizeof(int), cudaMemcpyDeviceToHost), "copy count") ||
+                !check(cudaMemcpy(out.data(), d_out, sizeof(T) * out.size(), cudaMemcpyDeviceToHost), "copy out") ||
+                !check(cudaMemcpy(mem.data(), d_mem, sizeof(int) * n, cudaMemcpyDeviceToHost), "copy membership"))
                 break;
-            }
-            cudaMemcpy(&nout, d_n, sizeof(int), cudaMemcpyDeviceToHost);
-            cudaMemcpy(out.data(), d_out, sizeof(T) * out.size(), cudaMemcpyDeviceToHost);
-            cudaMemcpy(mem.data(), d_mem, sizeof(int) * n, cudaMemcpyDeviceToHost);
+            if (nout < 0 || nout > n) st = fail(SCPHD_ERR_CUDA, "merge_components: output count out of range");
         } while (0);
         cudaFree(d_rows); cudaFree(d_out); cudaFree(d_flags); cudaFree(d_n); cudaFree(d_mem); cudaFree(d_sparse);
         if (st != SCPHD_OK) return st;

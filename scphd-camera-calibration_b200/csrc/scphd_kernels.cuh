@@ -1803,12 +1803,39 @@ __device__ __forceinline__ void resample_body(const Params& prm, double* lw, dou
         return;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    {   // argmax of the weights, first index on ties (the over-run fallback of .cu:2683-2693),
+        // as a block reduction: strided scans, then warps, then one warp over the warps
+        __shared__ double s_bw[32];
+        __shared__ int s_bi[32];
         double best = -1;
         int bi = -1;
-        for (int p = 0; p < N; ++p)
-            if (cum[p] > best) { best = cum[p]; bi = p; }
-        s_amax = bi < 0 ? 0 : bi;
+        for (int p = threadIdx.x; p < N; p += blockDim.x)
+            if (cum[p] > best) { best = cum[p]; bi = p; }   // NaN never wins, as in a serial scan
+        auto better = [](double w, int i, double bw, int bj) {
+            return i >= 0 && (bj < 0 || w > bw || (w == bw && i < bj));
+        };
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ow = __shfl_xor_sync(0xffffffffu, best, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (better(ow, oi, best, bi)) { best = ow; bi = oi; }
+        }
+        const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+        if (lane == 0) { s_bw[threadIdx.x >> 5] = best; s_bi[threadIdx.x >> 5] = bi; }
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            best = lane < nw ? s_bw[lane] : -1.0;
+            bi = lane < nw ? s_bi[lane] : -1;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ow = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (better(ow, oi, best, bi)) { best = ow; bi = oi; }
+            }
+            if (threadIdx.x == 0) s_amax = bi < 0 ? 0 : bi;
+        }
+    }
+    if (threadIdx.x == 0) {
         if (r0_override >= 0) {
             s_r0 = r0_override * (1.0 / N);
         } else {

@@ -6,9 +6,12 @@ in the reference tree, so OSPA follows its published definition, Schuhmacher, Vo
 and Vo, "A consistent metric for performance evaluation of multi-object filters",
 IEEE TSP 2008):
 
-* expected pose = weighted mean of the parent states (load_disparity_results.m:24-26);
-  calibration error = expected pose - true pose on the position (x,y,z) and angle
-  (theta, phi, psi) components (:66);
+* expected pose = weighted mean of the parent states (load_disparity_results.m:24-26),
+  the three angles as circular means (atan2 of the weighted sine and cosine sums, so
+  that parents either side of +-pi average to +-pi, not to 0); calibration error =
+  expected pose - true pose on the position (x,y,z) and angle (theta, phi, psi)
+  components (:66), each angle difference wrapped into [-pi, pi] as the reference's
+  wrapAngle does (src/device_math.cu:308-318);
 * the map of the MAP parent keeps the features of weight >= 0.33 (:31), cardinality =
   sum of weights (:32); each feature's sample cloud is projected into camera 1 and
   summarised by its mean (u, v, d) (:36-52);
@@ -47,15 +50,31 @@ def ospa(X: np.ndarray, Y: np.ndarray, c: float = 10.0, p: float = 1.0):
     return float(dist), float((loc / n) ** (1.0 / p)), float((card / n) ** (1.0 / p))
 
 
+ANGLES = slice(6, 9)   # theta, phi, psi of a 12-D parent state
+
+
+def wrap_angle(a):
+    """Angle(s) into [-pi, pi], as wrapAngle (src/device_math.cu:308-318): the
+    remainder of a / 2pi (sign of a), moved by 2pi when beyond pi."""
+    r = np.fmod(np.asarray(a, float), 2 * np.pi)
+    r = np.where(r > np.pi, r - 2 * np.pi, r)
+    return np.where(r < -np.pi, r + 2 * np.pi, r)
+
+
 def expected_pose(states: np.ndarray, log_weights: np.ndarray) -> np.ndarray:
+    """Weighted mean of the parent states; the angles as weighted circular means."""
     w = np.exp(log_weights - np.max(log_weights))
     w /= w.sum()
-    return (w[:, None] * states).sum(axis=0)
+    mean = (w[:, None] * states).sum(axis=0)
+    ang = states[:, ANGLES]
+    mean[ANGLES] = np.arctan2((w[:, None] * np.sin(ang)).sum(axis=0), (w[:, None] * np.cos(ang)).sum(axis=0))
+    return mean
 
 
 def calibration_error(states: np.ndarray, log_weights: np.ndarray, truth12: np.ndarray):
     e = expected_pose(states, log_weights) - truth12
-    return {"position_m": float(np.linalg.norm(e[0:3])), "angle_rad": float(np.linalg.norm(e[6:9])),
+    e[ANGLES] = wrap_angle(e[ANGLES])
+    return {"position_m": float(np.linalg.norm(e[0:3])), "angle_rad": float(np.linalg.norm(e[ANGLES])),
             "components": e[[0, 1, 2, 6, 7, 8]].tolist()}
 
 

@@ -1,8 +1,11 @@
-"""Generate the committed golden fixtures (run in a container that has the
-reference tree; the GPU box only reads the .npz files).
+"""Generate the committed golden fixtures (run where the reference tree is
+available, with REF_DIR pointing at it; the GPU box only reads the .npz files).
 
-disparity_sim_frames.npz  the first 12 measurement frames Z1/Z2 of the
-                          reference's data/disparity_sim.mat (2 x n, u;v),
+    REF_DIR=<reference tree> python tests/golden/make_golden.py
+
+disparity_sim_frames.npz  the first 100 measurement frames Z1/Z2 of the
+                          reference's data/disparity_sim.mat (2 x n, u;v) --
+                          max_steps of its shipped config/calibration.cfg --
                           and campose_2, read with scipy.
 ref_kernels.npz           inputs and outputs of the reference's OWN code
                           compiled for the host (oracle/_ref/libscphd_ref.so):
@@ -18,14 +21,21 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference"
+N_FRAMES = 100
+
+
+def ref_dir() -> str:
+    d = os.environ.get("REF_DIR")
+    if not d or not os.path.isfile(os.path.join(d, "src", "kernels.cu")):
+        sys.exit("make_golden.py needs REF_DIR=<reference tree holding src/kernels.cu and data/>")
+    return d
 
 
 def frames():
     import scipy.io as sio
-    m = sio.loadmat(os.path.join(REF, "data", "disparity_sim.mat"))
+    m = sio.loadmat(os.path.join(ref_dir(), "data", "disparity_sim.mat"))
     out = {"campose_2": m["campose_2"].ravel()}
-    for k in range(12):
+    for k in range(N_FRAMES):
         out["Z1_%d" % k] = np.asarray(m["Z1"][0, k], np.float64)
         out["Z2_%d" % k] = np.asarray(m["Z2"][0, k], np.float64)
     np.savez_compressed(os.path.join(HERE, "disparity_sim_frames.npz"), **out)
@@ -45,7 +55,7 @@ def packed(C):
 def ref_kernels():
     sys.path.insert(0, ROOT)
     from oracle import oracle as orc
-    orc.build(REF)
+    orc.build(ref_dir())
     ref = orc.RefLib()
     rng = np.random.default_rng(20240607)
     m8 = np.array([-895.6561, -891.2656, 400.0, 300.0, 5.0, 5.0, 0.95, 10.0001])

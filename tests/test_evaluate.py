@@ -29,6 +29,27 @@ def test_calibration_error_of_weighted_mean(pkg):
     assert e["position_m"] == pytest.approx(3.0)
 
 
+def test_calibration_angle_error_wraps(pkg, orc):
+    """Angles either side of +-pi: the truth at 3.1 rad and an estimate at -3.1 rad are
+    0.083 rad apart, not 6.2; the circular mean of parents at +3.13 and -3.13 is pi."""
+    ev = pkg.evaluate
+    st = np.zeros((1, 12))
+    st[0, 6:9] = [-3.1, 0.2, -3.1]
+    truth = np.zeros(12)
+    truth[6:9] = [3.1, 0.2, 3.1]
+    e = ev.calibration_error(st, np.zeros(1), truth)
+    gap = 2 * np.pi - 6.2
+    assert e["angle_rad"] == pytest.approx(np.sqrt(2) * gap, rel=1e-12)
+    assert e["components"][3] == pytest.approx(gap, rel=1e-12)
+    st = np.zeros((2, 12))
+    st[:, 6] = [3.13, -3.13]
+    pose = ev.expected_pose(st, np.log([0.5, 0.5]))
+    assert abs(ev.wrap_angle(pose[6] - np.pi)) < 1e-12
+    # the wrap agrees with the oracle's restatement of wrapAngle
+    for a in np.linspace(-20, 20, 101):
+        assert ev.wrap_angle(a) == pytest.approx(orc.wrap_angle(a), abs=1e-15)
+
+
 def test_metrics_on_an_oracle_run(pkg, orc):
     """A few dozen frames of a small scene through the oracle: the MAP map is populated,
     OSPA lies in [0, c] and the calibration error is finite.  (How well the filter as

@@ -160,23 +160,88 @@ def test_fp64_frames_match_oracle_certain_detection(pkg, orc):
 
 def test_reference_fixture_frames(pkg, orc):
     """The reference's own measurement frames (data/disparity_sim.mat, committed as
-    tests/golden/disparity_sim_frames.npz) with its shipped model parameters."""
+    tests/golden/disparity_sim_frames.npz) with its shipped model parameters and
+    particle counts (n_particles 100, particles_per_feature 100), for max_steps = 100
+    frames of its driver loop (src/main.cpp:73-97: predict(0.5), Z1 with the fixed
+    camera on even frames, Z2 on odd ones, resample).  The map capacity is set far
+    above the largest map of this run (596), so the cap never binds and the filter
+    is the reference's uncapped recurrence."""
     _need_gpu()
     import os
     g = np.load(os.path.join(os.path.dirname(__file__), "golden", "disparity_sim_frames.npz"))
     cfg = pkg.reference_defaults()
-    cfg.n_parents = 40
-    cfg.particles_per_feature = 64
-    cfg.max_gaussians = 256
+    assert cfg.n_parents == 100 and cfg.particles_per_feature == 100
+    cfg.max_gaussians = 1024
+    cfg.max_survivors = 640
     cfg.max_measurements = 64
+    cfg.precision = pkg.SCPHD_FP64
     gpu, ref = _pair(pkg, orc, cfg)
-    for k in range(6):
+    resampled = 0
+    for k in range(100):
         Z = g["Z1_%d" % k] if k % 2 == 0 else g["Z2_%d" % k]
         for f in (gpu, ref):
             f.predict(0.5)
             f.update(Z[0], Z[1], fixed_camera=(k % 2 == 0))
         _compare_frame(gpu, ref, Z.shape[1], k)
-        assert gpu.resample() == ref.resample()
+        rg, rr = gpu.resample(), ref.resample()
+        assert rg == rr, f"frame {k} resample decision"
+        if rr:
+            resampled += 1
+            assert np.array_equal(gpu.resample_indices(), ref.resample_indices()), f"frame {k} resample idx"
+    c = gpu.counters()
+    assert c[0] == 0 and c[1] == 0 and ref.truncations() == 0, f"capacity hit: {c[:2]}"
+    assert resampled > 0
+
+
+def _run_lockstep(pkg, gpu, ref, sc, n_frames):
+    """Step device and oracle together, comparing every frame; returns the number of
+    frames that resampled."""
+    resampled = 0
+    for k in range(n_frames):
+        z = sc.frames[k]
+        for f in (gpu, ref):
+            f.predict(pkg.scene.DT)
+            f.update(z[:, 0], z[:, 1], fixed_camera=sc.fixed[k], d=z[:, 2])
+        _compare_frame(gpu, ref, z.shape[0], k)
+        rg, rr = gpu.resample(), ref.resample()
+        assert rg == rr, f"frame {k} resample decision"
+        if rr:
+            resampled += 1
+            assert np.array_equal(gpu.resample_indices(), ref.resample_indices()), f"frame {k} resample idx"
+    return resampled
+
+
+def test_fp64_capped_maps_match_oracle(pkg, orc):
+    """The map capacity binds: the plain_c1 scene (200 landmarks, clutter 50/frame,
+    (u,v,d), <= 256 Gaussians per parent, 100 samples per Gaussian) on 48 parents for
+    14 frames.  The cap first binds at frame 5 and then cuts most parents' maps every
+    frame; device and oracle must keep the same entries (map sizes exact, every
+    value within the FP64 tolerances) and count the same truncations."""
+    _need_gpu()
+    sc, cfg = pkg.scene.workload("plain_c1", precision=pkg.SCPHD_FP64, n_frames=14)
+    cfg.n_parents = 48
+    gpu, ref = _pair(pkg, orc, cfg)
+    _run_lockstep(pkg, gpu, ref, sc, sc.n_frames)
+    c = gpu.counters()
+    assert ref.truncations() > 100, ref.truncations()
+    assert c[0] == ref.truncations(), (int(c[0]), ref.truncations())
+    assert c[1] == 0, "survivor scratch overflow"
+
+
+def test_fp64_config0_all_frames_match_oracle(pkg, orc):
+    """BASELINE config 0 in full: 256 parents, 50 landmarks, clutter 10/frame,
+    <= 64 Gaussians per parent, 100 samples per Gaussian, all 100 frames, FP64,
+    compared with the oracle after every frame.  The cap binds on every parent from
+    about frame 10 on."""
+    _need_gpu()
+    sc, cfg = pkg.scene.workload("plain_c0", precision=pkg.SCPHD_FP64)
+    assert cfg.n_parents == 256 and cfg.max_gaussians == 64 and sc.n_frames == 100
+    gpu, ref = _pair(pkg, orc, cfg)
+    resampled = _run_lockstep(pkg, gpu, ref, sc, sc.n_frames)
+    c = gpu.counters()
+    assert c[0] == ref.truncations() and ref.truncations() > 0
+    assert c[1] == 0
+    assert resampled > 0
 
 
 def test_merge_decisions_identical_inputs(pkg, orc):

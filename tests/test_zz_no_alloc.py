@@ -58,7 +58,9 @@ def _components(rng, n):
 
 
 @pytest.mark.parametrize("prec", [1, 0])
-def test_static_merge_equals_allocating_merge(pkg, prec):
+def test_static_merge_equals_allocating_merge(pkg, orc, prec):
+    """Both entry points, and the FP64 oracle's greedy merge, on the largest list the
+    static entry point accepts and then a small one."""
     if not gpu_available():
         pytest.skip("no CUDA device")
     _, fn = _static_fn(pkg)
@@ -75,6 +77,10 @@ def test_static_merge_equals_allocating_merge(pkg, prec):
         assert np.array_equal(mem_s, mem_a)
         tol = dict(rtol=1e-10, atol=1e-10) if prec == 1 else dict(rtol=2e-4, atol=2e-4)
         np.testing.assert_allclose(out_s, out_a, **tol)
+        out_o, mem_o = orc.merge(comps, flags, 6.0)
+        assert out_s.shape == out_o.shape, f"n={n}: {out_s.shape} vs oracle {out_o.shape}"
+        assert np.array_equal(mem_s, mem_o), f"n={n}: membership differs from the oracle"
+        np.testing.assert_allclose(out_s, out_o, **tol)
 
 
 def test_static_merge_rejects_oversize(pkg):
