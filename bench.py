@@ -410,16 +410,50 @@ def run_b200(args):
                      "fitted_per_parent_frame": float(c1[10] - c0[10]) / (K * cfg.n_parents),
                      "merged_per_parent_frame": float(c1[11] - c0[11]) / (K * cfg.n_parents)},
     }
-    print(json.dumps(line), flush=True)
     filt.close()
+    if world == 1 and not args.no_extras:
+        line.update(extra_workloads(args, pkg))
+    print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
+
+
+def extra_workloads(args, pkg):
+    """Short runs of the many-filter and serving workloads, reported beside the
+    single-filter line: 64 filters of the plain_c0 shape (256 parents, <= 64
+    Gaussians, 50 landmarks, clutter 10) batched against the same filters stepped one
+    at a time, and a serving window of Poisson arrivals with per-frame latencies."""
+    import copy
+    import torch
+    out = {}
+    a = copy.copy(args)
+    a.workload, a.filters, a.steps, a.warmup, a.prefill = "batched_c0x64", 64, 10, 3, 20
+    r = run_batched(a, pkg)
+    out["batched_c0x64"] = {
+        "value": r["batched"]["value"], "unit": UNIT, "plain_value": r["plain"]["value"],
+        "batched_over_plain": r["batched_over_plain"], "filters": r["filters"], "parents": r["parents"],
+        "waves": r["waves"], "frame_ms": r["wave_frame_ms"], "steps": r["batched"]["steps"],
+        "e2e": r["e2e"]["value"], "gpu_launches": r["gpu_launches"],
+        "note": "batched = one batch step per frame for all 64 filters (graph-replayed); plain = the same "
+                "filters stepped one after another; frames alternate in pairs so both see maps of one size"}
+    torch.cuda.empty_cache()
+    a = copy.copy(args)
+    a.serve_seconds = args.extra_serve_seconds
+    sv = run_serving(a, pkg)
+    out["serving_c4"] = {
+        "value": sv["value"], "unit": UNIT, "window_s": sv["config"]["window_s"],
+        "frame_latency_ms": sv["frame_latency_ms"], "admission_wait_s": sv["admission_wait_s"],
+        "jobs_admitted": sv["config"]["admitted"], "jobs_completed": sv["config"]["completed"],
+        "mean_jobs_per_step": sv["mean_jobs_per_step"], "device_busy_fraction": sv["device_busy_fraction"],
+        "note": "Poisson arrivals at 20 jobs/s from an empty server; value = updates over the wall-clock "
+                "window; latency = device time of the batched step that advanced a job's frame"}
+    return out
 
 
 def run_batched(args, pkg, quiet=False):
     """Many-filter workload: 64 filters of uneven size (batched_specs), grouped into
     device-resident waves under an 80% HBM budget.  Each wave is one SCPHDBatch
-    stepped from a captured CUDA graph (six kernels per frame for all its filters).
+    stepped from a captured CUDA graph (seven kernels per frame for all its filters).
     Timed per wave: K pairs of batched frames alternating with K pairs of frames in
     which the same filters are stepped plain, one filter at a time (device events on
     the batch stream), then K batched frames end to end from host arrays with the
@@ -495,7 +529,7 @@ def run_batched(args, pkg, quiet=False):
                 if form == "b":
                     res["frame_ms"] += [e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])]
                     res["truncations"] += sum(int(b[0] - a[0]) for a, b in zip(c0, c1))
-                    lb += 12
+                    lb += 14   # seven kernels per batched frame, two frames
         res["launches"] += lb
         res["overflows"] += sum(int(f.counters()[1]) for f in fs)
         # end to end: host frames in, parent states out, through the public API
@@ -812,6 +846,8 @@ def main():
     ap.add_argument("--cpu-prefill", type=int, default=30)
     ap.add_argument("--cpu-frames", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the short batched and serving runs")
+    ap.add_argument("--extra-serve-seconds", type=float, default=20.0, help="serving window of the extra run")
     ap.add_argument("--parents", type=int, default=0, help="override the parent count (profiling only)")
     ap.add_argument("--filters", type=int, default=64, help="filters of the batched_c2 workload")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="serving window of serving_c4")

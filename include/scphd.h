@@ -193,7 +193,8 @@ void* scphd_stream(scphd_filter* f);
 
 /* Per-stage device timing with CUDA events recorded on the handle's stream around
  * each stage's kernel (off by default).  Stages: 0 parent prediction, 1 cloud
- * fit, 2 likelihood/survivors, 3 merge, 4 parent weights, 5 resampling.
+ * fit, 2 likelihood/survivors, 3 merge, 4 parent weights, 5 resampling, 6 Kalman
+ * terms of the fitted Gaussians.
  * scphd_get_stage_times synchronises the stream, returns the summed milliseconds
  * and launch counts per stage since the last call, and clears them. */
 scphd_status scphd_set_profiling(scphd_filter* f, int32_t enable);
@@ -245,7 +246,7 @@ scphd_status scphd_device_bytes(const scphd_config* cfg, int64_t* bytes);
 
 /* ------------------------------------------------------------------ batches
  * Many filters advanced together: every batched step runs predict(dt) + update +
- * resample for all member filters with one kernel launch per stage (six per frame,
+ * resample for all member filters with one kernel launch per stage (seven per frame,
  * whatever the number of filters), each launch covering every filter's parents
  * through a block -> (filter, parent) map.  Member filters must share device,
  * precision and meas_dim; they may differ in size.  While in a batch, the filters

@@ -76,6 +76,7 @@ def lib():
             "orc_get_survivors": (None, [VP, P(I32)]),
             "orc_get_resample_indices": (None, [VP, P(I32)]),
             "orc_philox": (None, [P(U32), P(U32), P(U32)]),
+            "orc_philox_rounds": (None, [P(U32), P(U32), I32, P(U32)]),
             "orc_normals4": (None, [U64, U32, U32, U32, U32, P(D)]),
             "orc_ctr_word3": (U32, [I32, I32, I32]),
             "orc_merge": (None, [P(D), P(U8), I32, D, P(D), P(I32), P(I32)]),
@@ -89,6 +90,8 @@ def lib():
             "orc_detect": (None, [VP, P(D), P(D), P(D)]),
             "orc_cap_keep": (None, [P(D), I32, I32, P(U8)]),
             "orc_truncations": (ctypes.c_int64, [VP]),
+            "orc_precut_weights": (I32, [VP, I32, P(D)]),
+            "orc_unit_weight_fits": (ctypes.c_int64, [VP]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(L, name)
@@ -197,6 +200,18 @@ class Oracle:
         lib().orc_get_survivors(self._h, _i(s))
         return s
 
+    def precut_weights(self, p):
+        """Entry weights of parent p's new map before the capacity cut (last update)."""
+        n = lib().orc_precut_weights(self._h, p, None)
+        w = np.zeros(n)
+        if n:
+            lib().orc_precut_weights(self._h, p, _d(w))
+        return w
+
+    def unit_weight_fits(self) -> int:
+        """In-view clouds fitted with unit weights (all their weights were 0) since create."""
+        return int(lib().orc_unit_weight_fits(self._h))
+
     def truncations(self) -> int:
         """Maps cut at max_gaussians since create."""
         return int(lib().orc_truncations(self._h))
@@ -225,10 +240,19 @@ class Oracle:
 
 
 def philox(ctr, key):
+    """The generator of the random streams (Philox4x32, 7 rounds)."""
     c = (U32 * 4)(*ctr)
     k = (U32 * 2)(*key)
     o = (U32 * 4)()
     lib().orc_philox(c, k, o)
+    return list(o)
+
+
+def philox_rounds(ctr, key, rounds):
+    c = (U32 * 4)(*ctr)
+    k = (U32 * 2)(*key)
+    o = (U32 * 4)()
+    lib().orc_philox_rounds(c, k, int(rounds), o)
     return list(o)
 
 

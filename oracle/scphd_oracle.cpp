@@ -24,7 +24,7 @@
 //   resample           src/scphdcameracalibration.cu:2641-2817
 //
 // Deliberate differences from the reference, all shared with the device code:
-//   * random numbers come from Philox4x32-10 streams keyed by
+//   * random numbers come from Philox4x32-7 streams keyed by
 //     (seed, frame, stage, parent, gaussian, sample) with Box-Muller normals,
 //     instead of time()-seeded minstd engines (src/scphdcameracalibration.cu:1047-1118);
 //   * reductions are sequential left-to-right in FP64;
@@ -33,7 +33,9 @@
 //   * meas_dim 3 generalises H = [I_2 0] to [I_3 0] and births take the measured d;
 //   * a stereo baseline multiplies d and vd (baseline 1 is the reference);
 //   * a parent's map is capped at max_gaussians entries, keeping the largest
-//     weights (the reference's maps are unbounded).
+//     weights (the reference's maps are unbounded);
+//   * the merge's argmax compares weights rounded to single precision (equal keys
+//     are ties, ordered by the reference's index rule), as does the capacity cut.
 #include "scphd.h"
 
 #include <algorithm>
@@ -55,10 +57,15 @@ const double kPi = M_PI;
 // ---------------------------------------------------------------- random streams
 enum Stage { ST_PRIOR = 1, ST_CAM = 2, ST_FEAT = 3, ST_SAMPLE = 4, ST_RESAMPLE = 5 };
 
-void philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2], uint32_t out[4]) {
+// Philox4x32 (Salmon, Moraes, Dror and Shaw, SC'11) with R rounds.  The streams use
+// kPhiloxRounds = 7 rounds, the fewest the authors report passing TestU01's BigCrush;
+// R = 10 is the Random123 default whose known-answer vectors pin the round function.
+const int kPhiloxRounds = 7;
+
+void philox4x32(const uint32_t ctr_in[4], const uint32_t key_in[2], uint32_t out[4], int rounds) {
     uint32_t c0 = ctr_in[0], c1 = ctr_in[1], c2 = ctr_in[2], c3 = ctr_in[3];
     uint32_t k0 = key_in[0], k1 = key_in[1];
-    for (int r = 0; r < 10; ++r) {
+    for (int r = 0; r < rounds; ++r) {
         uint64_t p0 = (uint64_t)0xD2511F53u * c0;
         uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
         uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
@@ -82,7 +89,7 @@ struct Stream {
     void words(uint32_t s, uint32_t j, uint32_t p, uint32_t c3, uint32_t w[4]) const {
         const uint32_t ctr[4] = {s, j, p, c3};
         const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
-        philox4x32_10(ctr, key, w);
+        philox4x32(ctr, key, w, kPhiloxRounds);
     }
     // four standard normals from one Philox block (two Box-Muller pairs)
     void normals4(uint32_t s, uint32_t j, uint32_t p, uint32_t c3, double z[4]) const {
@@ -217,6 +224,14 @@ uint32_t tie_key(uint32_t r) {
     return (rev << 24) | (r >> 8);
 }
 
+// Order key of a weight in the greedy merge's argmax and in the map-capacity cut: the
+// weight rounded to single precision.  Exact ties are common (every birth of an
+// unexplained measurement has weight w0 / (M w0 + kappa)) and so are FP64 weights that
+// differ only in their last bits (a Gaussian term 1e-15 of a normaliser); any two
+// implementations of the FP64 sums order such near-ties differently, so equal
+// single-precision keys count as ties and the index rules order them.
+inline float order_key(double w) { return (float)w; }
+
 // greedy merge of src/kernels.cu:662-874 on one map
 void merge_map(const std::vector<G6>& comps, std::vector<uint8_t>& flags, double min_sep,
                std::vector<G6>& out, std::vector<int>* member_of) {
@@ -227,9 +242,8 @@ void merge_map(const std::vector<G6>& comps, std::vector<uint8_t>& flags, double
         int best = -1;
         for (int i = 0; i < n; ++i) {
             if (flags[i]) continue;
-            if (best < 0 || comps[best].w < comps[i].w ||
-                (comps[best].w == comps[i].w && tie_key(i) < tie_key(best)))
-                best = i;
+            const float kb = best < 0 ? 0.f : order_key(comps[best].w), ki = order_key(comps[i].w);
+            if (best < 0 || kb < ki || (kb == ki && tie_key(i) < tie_key(best))) best = i;
         }
         if (best < 0) break;
         const G6 maxF = comps[best];
@@ -265,12 +279,14 @@ void merge_map(const std::vector<G6>& comps, std::vector<uint8_t>& flags, double
     }
 }
 
-// Entries kept when a map of weights w is cut to cap entries: the cap largest
-// weights, equal weights in entry order (a stable sort by decreasing weight).
+// Entries kept when a map of weights w is cut to cap entries: the cap largest order
+// keys (weights rounded to single precision), equal keys in entry order (a stable
+// sort by decreasing key).
 void cap_keep(const std::vector<double>& w, int cap, std::vector<char>& keep) {
     std::vector<int> order(w.size());
     for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return w[a] > w[b]; });
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return order_key(w[a]) > order_key(w[b]); });
     keep.assign(w.size(), 0);
     for (int i = 0; i < cap && i < (int)w.size(); ++i) keep[order[i]] = 1;
 }
@@ -310,6 +326,7 @@ struct Oracle {
     int frame = 0;
     int weight_mode = 0;   // 0 log domain, 1 linear as written
     long long truncations = 0;   // maps cut at max_gaussians since create
+    long long unit_weight_fits = 0;   // in-view clouds whose weights were all 0 (fitted with weights 1)
     std::vector<Ext> ext;
     std::vector<double> lw;          // log weights (mode 0) or linear weights (mode 1)
     std::vector<std::vector<Cloud>> maps;
@@ -321,6 +338,7 @@ struct Oracle {
     std::vector<double> ell, loglik;
     std::vector<int> resample_idx;
     std::vector<int> survivors;
+    std::vector<std::vector<double>> precut;   // entry weights of each new map before the cap
 
     explicit Oracle(const scphd_config& c) : cfg(c) {
         rng.seed = c.seed;
@@ -515,8 +533,10 @@ struct Oracle {
     // non-detection clouds in Gaussian order) holds more, the max_gaussians entries of
     // largest weight are kept, equal weights in entry order, and the kept entries
     // keep their order.  max_gaussians <= 0 means no cap.
-    void cap_map(std::vector<Cloud>& out) {
+    void cap_map(std::vector<Cloud>& out, std::vector<double>& precut) {
         const int cap = cfg.max_gaussians;
+        precut.resize(out.size());
+        for (size_t i = 0; i < out.size(); ++i) precut[i] = out[i].W;
         if (cap <= 0 || (int)out.size() <= cap) return;
         std::vector<double> w(out.size());
         for (size_t i = 0; i < out.size(); ++i) w[i] = out[i].W;
@@ -545,6 +565,7 @@ struct Oracle {
         ell.assign((size_t)N * M, 0.0);
         loglik.assign(N, 0.0);
         survivors.assign(N, 0);
+        precut.assign(N, {});
         const double bpc = safe_log(M * cfg.w0 + cfg.kappa);   // .cu:1744-1745
         const double log_w0 = safe_log(cfg.w0);
         const Ext zero_ext = {{0, 0, 0, 0, 0, 0}, {0, 0, 0, 0, 0, 0}};
@@ -573,6 +594,10 @@ struct Oracle {
                 }
                 double sum = 0;
                 for (int s = 0; s < P; ++s) sum += om[s];
+                if (sum == 0 && n_in > 0) {   // every weight becomes exp(LOG0 - LOG0) = 1
+#pragma omp atomic
+                    ++unit_weight_fits;
+                }
                 for (int s = 0; s < P; ++s) om[s] = std::exp(safe_log(om[s]) - safe_log(sum));
                 G6& g = fit[j];
                 g.w = cl.W;
@@ -692,7 +717,7 @@ struct Oracle {
                 c.x.swap(X6);
                 out.push_back(std::move(c));
             }
-            cap_map(out);
+            cap_map(out, precut[p]);
             mp.swap(out);
         }
         if (!fixed) {   // parent weights, .cu:1813-1876
@@ -851,7 +876,12 @@ void orc_get_resample_indices(void* h, int* idx) {
 }
 
 // ---- stand-alone stages
-void orc_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) { philox4x32_10(ctr, key, out); }
+void orc_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    philox4x32(ctr, key, out, kPhiloxRounds);
+}
+void orc_philox_rounds(const uint32_t ctr[4], const uint32_t key[2], int rounds, uint32_t out[4]) {
+    philox4x32(ctr, key, out, rounds);
+}
 void orc_normals4(uint64_t seed, uint32_t s, uint32_t j, uint32_t p, uint32_t c3, double z[4]) {
     Stream st{seed};
     st.normals4(s, j, p, c3, z);
@@ -893,6 +923,14 @@ void orc_cap_keep(const double* w, int n, int cap, uint8_t* keep) {
     for (int i = 0; i < n; ++i) keep[i] = (uint8_t)k[i];
 }
 long long orc_truncations(void* h) { return static_cast<Oracle*>(h)->truncations; }
+long long orc_unit_weight_fits(void* h) { return static_cast<Oracle*>(h)->unit_weight_fits; }
+// entry weights of parent p's new map before the capacity cut (last update); returns
+// the count, writes them when out is not null
+int orc_precut_weights(void* h, int p, double* out) {
+    const std::vector<double>& w = static_cast<Oracle*>(h)->precut[p];
+    if (out) std::memcpy(out, w.data(), w.size() * sizeof(double));
+    return (int)w.size();
+}
 
 // world -> disparity of one point with extrinsic e (12), using the filter's model
 void orc_measure(void* h, const double* X, const double* e12, double* y) {

@@ -31,11 +31,13 @@ __host__ __device__ inline uint32_t ctr_word3(uint32_t frame, uint32_t stage, ui
     return (frame << 12) | (stage << 8) | block;
 }
 
-// Philox4x32-10 (Salmon et al., SC'11), counter (s, j, p, c3), key = seed
+// Philox4x32 (Salmon, Moraes, Dror and Shaw, SC'11) with 7 rounds, the fewest the
+// authors report passing TestU01's BigCrush; counter (s, j, p, c3), key = seed
+constexpr int kPhiloxRounds = 7;
 __host__ __device__ inline void philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
                                        uint32_t k0, uint32_t k1, uint32_t out[4]) {
 #pragma unroll
-    for (int r = 0; r < 10; ++r) {
+    for (int r = 0; r < kPhiloxRounds; ++r) {
         // one 32x32 -> 64-bit product per multiplier gives both halves
         const uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
         const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
@@ -52,7 +54,7 @@ __host__ __device__ inline void philox(uint32_t c0, uint32_t c1, uint32_t c2, ui
 __device__ __forceinline__ void philox_rk(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, const uint32_t* rk,
                                           uint32_t out[4]) {
 #pragma unroll
-    for (int r = 0; r < 10; ++r) {
+    for (int r = 0; r < kPhiloxRounds; ++r) {
         const uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
         const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
         const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
@@ -525,7 +527,22 @@ __device__ inline void kalman_prep(T w, T pdbar, const T* P, const Model& m, T* 
         Kg[q] = acc;
         dst[kPrepK + q] = acc;
     }
-    // Joseph entry e = (ea, eb), ea >= eb
+    // Joseph form with the shared products hoisted: with A = P H' (A_bk = P[b][k]) and
+    // Q = K S (Q_bk = sum_l K_bl S_lk, S = H P H' + R), the entry (ea, eb), ea >= eb, of
+    // (I - K H) P (I - K H)' + K R K' is P_ab - sum_k K_ak A_bk - sum_k A_ak K_bk
+    // + sum_k K_ak Q_bk (the last sum is (K (H P H' + R) K')_ab).
+    T Q[18];
+#pragma unroll
+    for (int r = 0; r < 6; ++r)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            T acc = 0;
+            if (k < K) {
+#pragma unroll
+                for (int l = 0; l < K; ++l) acc += Kg[r * 3 + l] * (l == k ? S[tri(l, k)] : P[tri(l, k)]);
+            }
+            Q[r * 3 + k] = acc;
+        }
 #pragma unroll
     for (int ea = 0; ea < 6; ++ea)
 #pragma unroll
@@ -537,9 +554,7 @@ __device__ inline void kalman_prep(T w, T pdbar, const T* P, const Model& m, T* 
             const T Kak = Kg[ea * 3 + k], Kbk = Kg[eb * 3 + k];
             sv -= Kak * P[tri(k, eb)];
             sv -= P[tri(ea, k)] * Kbk;
-            sv += Kak * (T)m.var[k] * Kbk;
-#pragma unroll
-            for (int l = 0; l < K; ++l) sv += Kak * P[tri(k, l)] * Kg[eb * 3 + l];
+            sv += Kak * Q[eb * 3 + k];
         }
         Pn[e] = sv;
         dst[kPrepCov + e] = sv;

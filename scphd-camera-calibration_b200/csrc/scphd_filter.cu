@@ -232,6 +232,7 @@ public:
         }
         b.fit = a.take<T>(N * G * kRow);
         b.prep = a.take<T>(N * G * kPrep);
+        b.lik = a.take<T>(N * G * kLikTerms);
         b.z = a.take<T>(Mc * 3);
         b.ell = a.take<T>(N * Mc);
         b.surv_r = a.take<int>(N * S);
@@ -282,10 +283,12 @@ public:
             CUDA_TRY(allow_dynamic_smem((const void*)k_merge<T, 2>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit<T, 2>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_likelihood<T, 2>));
+            CUDA_TRY(allow_dynamic_smem((const void*)k_prep<T, 2>));
         } else {
             CUDA_TRY(allow_dynamic_smem((const void*)k_merge<T, 3>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit<T, 3>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_likelihood<T, 3>));
+            CUDA_TRY(allow_dynamic_smem((const void*)k_prep<T, 3>));
         }
         const int N = prm.N;
         k_prior<<<(N + 255) / 256, 256, 0, stream>>>(prm, b.ext, b.lw);
@@ -333,6 +336,10 @@ public:
         k_cloud_fit<T, K><<<N, 256, fit_smem, stream>>>(prm, b, cur, M, fixed, pending ? 1 : 0, pending_dt, pending_frame,
                                                   sample_frame[cur], M > 0 ? d_stage : nullptr,
                                                   M > 0 ? d_stage + M : nullptr, M > 0 ? d_stage + 2 * M : nullptr);
+        LAUNCHED();
+        stage_end(h);
+        h = stage_begin(6);
+        k_prep<T, K><<<N, kPrepThreads, prep_smem_bytes<T>(), stream>>>(prm, b, cur);
         LAUNCHED();
         stage_end(h);
         pending = false;
@@ -604,7 +611,7 @@ Params make_params(const scphd_config& c) {
     for (int i = 0; i < 12; ++i) { p.prior_a[i] = c.prior_a[i]; p.prior_b[i] = c.prior_b[i]; }
     p.key0 = (uint32_t)c.seed;
     p.key1 = (uint32_t)(c.seed >> 32);
-    for (int r = 0; r < 10; ++r) {   // Philox round keys
+    for (int r = 0; r < kPhiloxRounds; ++r) {   // Philox round keys
         p.rk[2 * r] = p.key0 + 0x9E3779B9u * (uint32_t)r;
         p.rk[2 * r + 1] = p.key1 + 0xBB67AE85u * (uint32_t)r;
     }
@@ -1129,7 +1136,7 @@ namespace {
 
 template <typename T> struct Batch final : scphd_batch {
     // Filters are launched in groups of up to kBatchSlots, each group with its own
-    // parameter table and block maps; six launches per group and frame.
+    // parameter table and block maps; seven launches per group and frame.
     struct Group {
         int first = 0, count = 0;       // filters [first, first + count)
         SlotTable<T>* tab = nullptr;    // host copy, passed by value at each launch
@@ -1253,10 +1260,12 @@ template <typename T> struct Batch final : scphd_batch {
             CUDA_TRY(allow_dynamic_smem((const void*)k_merge_batch<T, 2>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit_batch<T, 2>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_likelihood_batch<T, 2>));
+            CUDA_TRY(allow_dynamic_smem((const void*)k_prep_batch<T, 2>));
         } else {
             CUDA_TRY(allow_dynamic_smem((const void*)k_merge_batch<T, 3>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit_batch<T, 3>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_likelihood_batch<T, 3>));
+            CUDA_TRY(allow_dynamic_smem((const void*)k_prep_batch<T, 3>));
         }
         // members now issue on the batch stream
         for (scphd_filter* f : fs) {
@@ -1276,6 +1285,11 @@ template <typename T> struct Batch final : scphd_batch {
         }
         for (const Group& g : groups) {
             k_cloud_fit_batch<T, KK><<<g.n_parent, 256, fit_smem, stream>>>(*g.tab, d_fa + g.first, g.map_parent);
+            LAUNCHED();
+        }
+        for (const Group& g : groups) {
+            k_prep_batch<T, KK><<<g.n_parent, kPrepThreads, prep_smem_bytes<T>(), stream>>>(*g.tab, d_fa + g.first,
+                                                                                               g.map_parent);
             LAUNCHED();
         }
         for (const Group& g : groups) {
@@ -1304,7 +1318,7 @@ template <typename T> struct Batch final : scphd_batch {
         return SCPHD_OK;
     }
 
-    int launches_per_frame() const { return 6 * (int)groups.size(); }
+    int launches_per_frame() const { return 7 * (int)groups.size(); }
 
     scphd_status tune_collect() {
         if (tune_pending < 0) return SCPHD_OK;

@@ -6,8 +6,9 @@
 //                           components) or load (non-detection clouds) the sample
 //                           cloud, apply the pending feature prediction, transform
 //                           world->disparity, pD per sample, refit mean/cov, write
-//                           the retained non-detection cloud and the Gaussian's
-//                           measurement-independent Kalman terms        [N CTAs]
+//                           the candidate non-detection cloud            [N CTAs]
+//   k_prep              (c0) per fitted Gaussian: measurement-independent Kalman
+//                           terms (S^-1, log-constant, gain, posterior, PD flag) [N x 128]
 //   k_likelihood        (c) per (parent, measurement): log-sum-exp over the
 //                           parent's Gaussians (the normaliser), then survivors
 //                           (w >= min_weight and PD) compacted per parent [N x M/128]
@@ -45,7 +46,8 @@ template <typename T> struct Bufs {
     double* map_ext[2]; // N x 12: extrinsic the merged components are sampled with
     T* cloud[2];        // N*Gcap clouds of 7 x Ps (x,y,z,vx,vy,vz,omega)
     T* fit;             // N*Gcap rows of kRow
-    T* prep;            // N*Gcap rows of kPrep
+    T* prep;            // N*Gcap rows of kPrep (gain and posterior, read by the merge)
+    T* lik;             // N*Gcap rows of kLikTerms (the likelihood's per-Gaussian terms)
     T* z;               // Mcap x 3 measurements
     T* ell;             // N x Mcap normalisers
     int* surv_r;        // N x Scap survivor ranks
@@ -238,9 +240,7 @@ constexpr int kFitWarps = 8;
 constexpr int kStageRows = 8;   // r d[6], r, w'
 template <typename T> __host__ __device__ inline size_t cloud_fit_smem_bytes(int P) {
     const int P4 = (P + 3) & ~3;
-    const size_t stage = (size_t)kFitWarps * 2 * (kStageRows * stage_stride<T>(P4) + 16);   // sample rows
-    const size_t prep = (size_t)kFitWarps * 32 * 42;                                  // per-thread Kalman scratch
-    return (stage > prep ? stage : prep) * sizeof(T);
+    return (size_t)kFitWarps * 2 * (kStageRows * stage_stride<T>(P4) + 16) * sizeof(T);   // sample rows
 }
 
 template <typename T, int K>
@@ -488,18 +488,6 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
         }
     }
     __syncthreads();
-    // measurement-independent Kalman terms, one thread per fitted Gaussian; the fitted
-    // covariance and the posterior are staged in the (now free) sample rows
-    {
-        T* sPk = s_stage + (size_t)threadIdx.x * 42;
-        for (int j = threadIdx.x; j < G; j += blockDim.x) {
-            const T* fr = b.fit + ((size_t)p * prm.Gcap + j) * kRow;
-#pragma unroll
-            for (int q = 0; q < 21; ++q) sPk[q] = fr[8 + q];
-            kalman_prep<T, K>(fr[0], fr[1], sPk, m, sPk + 21, b.prep + ((size_t)p * prm.Gcap + j) * kPrep);
-        }
-    }
-    __syncthreads();
     if (threadIdx.x == 0) {
         atomicAdd(&b.counters[8], (unsigned long long)s_rd);
         atomicAdd(&b.counters[9], (unsigned long long)s_wr);
@@ -528,6 +516,93 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
                          fa.sample_frame, fa.zu, fa.zv, fa.zd, fp.y, reinterpret_cast<T*>(dsm_fit));
 }
 
+// ---------------------------------------------------------------- (c0) Kalman terms
+// Measurement-independent Kalman terms of every fitted Gaussian (kalman_prep: S, S^-1,
+// log-constant, gain, Joseph posterior and its PD test; src/kernels.cu:506-598), one
+// thread per Gaussian, in a launch of its own between the cloud fit and the likelihood
+// (each thread runs one long dependent chain; here the warps of many parents hide each
+// other's latency).  Each thread reads its fitted row in 16-byte pieces and writes its
+// rows into shared memory (odd strides: no bank conflicts); the block then copies the
+// rows of its Gaussians -- contiguous in global memory -- out with coalesced stores:
+//   prep row (kPrep): the gain and posterior covariance the merge reads per survivor;
+//   likelihood row (kLikTerms): log-constant (-inf when the posterior is not PD), PD
+//   flag, packed S^-1, mean (u, v, d) -- the k_likelihood terms, read in 16-byte pieces.
+constexpr int kLikTerms = 12;   // log-constant, PD flag, S^-1 (6), mean (3), pad: 16-byte pieces
+constexpr int kPrepThreads = 128;
+constexpr int kPrepStride = kPrep + 1, kLikStride = kLikTerms + 1;
+template <typename T> __host__ __device__ inline size_t prep_smem_bytes() {
+    return (size_t)kPrepThreads * (kPrepStride + kLikStride) * sizeof(T);
+}
+
+__device__ __forceinline__ void load_row29(const float* fr, float v[29]) {   // fitted row: 16-byte pieces
+    const float4* q = reinterpret_cast<const float4*>(fr);
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+        const float4 x = q[i];
+        v[4 * i] = x.x; v[4 * i + 1] = x.y; v[4 * i + 2] = x.z; v[4 * i + 3] = x.w;
+    }
+    v[28] = fr[28];
+}
+__device__ __forceinline__ void load_row29(const double* fr, double v[29]) {
+    const double2* q = reinterpret_cast<const double2*>(fr);
+#pragma unroll
+    for (int i = 0; i < 14; ++i) {
+        const double2 x = q[i];
+        v[2 * i] = x.x; v[2 * i + 1] = x.y;
+    }
+    v[28] = fr[28];
+}
+
+template <typename T, int K>
+__device__ __forceinline__ void prep_body(const Params& prm, const Bufs<T>& b, int cur, int p, T* smem) {
+    const int G = min(b.map_n[cur][b.src[p]], prm.Gcap);
+    T* s_prep = smem;                                     // kPrepThreads rows of kPrepStride
+    T* s_lik = smem + (size_t)kPrepThreads * kPrepStride;  // kPrepThreads rows of kLikStride
+    for (int j0 = 0; j0 < G; j0 += kPrepThreads) {
+        const int n = min(kPrepThreads, G - j0);
+        if ((int)threadIdx.x < n) {
+            T v[29];
+            load_row29(b.fit + ((size_t)p * prm.Gcap + j0 + threadIdx.x) * kRow, v);
+            T Pn[21];
+            T* d = s_prep + (size_t)threadIdx.x * kPrepStride;
+            kalman_prep<T, K>(v[0], v[1], v + 8, prm.model, Pn, d);
+            d[kPrep - 1] = T(0);
+            T* l = s_lik + (size_t)threadIdx.x * kLikStride;
+            // a non-PD posterior's log-constant is staged as -inf (its weight is LOG0 before
+            // the normaliser, kernels.cu:597-598), so the normaliser pass needs no test
+            l[0] = (d[0] > tneg_inf<T>() && d[1] != T(0)) ? d[0] : tneg_inf<T>();
+            l[1] = d[1];
+#pragma unroll
+            for (int i = 0; i < 6; ++i) l[2 + i] = d[kPrepSi + i];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) l[8 + a] = v[2 + a];
+            l[11] = T(0);
+        }
+        __syncthreads();
+        T* gp = b.prep + ((size_t)p * prm.Gcap + j0) * kPrep;
+        for (int e = threadIdx.x; e < n * kPrep; e += kPrepThreads) gp[e] = s_prep[(e / kPrep) * kPrepStride + e % kPrep];
+        T* gl = b.lik + ((size_t)p * prm.Gcap + j0) * kLikTerms;
+        for (int e = threadIdx.x; e < n * kLikTerms; e += kPrepThreads)
+            gl[e] = s_lik[(e / kLikTerms) * kLikStride + e % kLikTerms];
+        __syncthreads();
+    }
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kPrepThreads) k_prep(__grid_constant__ const Params prm,
+                                                       __grid_constant__ const Bufs<T> b, int cur) {
+    extern __shared__ __align__(16) unsigned char dsm_prep[];
+    prep_body<T, K>(prm, b, cur, blockIdx.x, reinterpret_cast<T*>(dsm_prep));
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kPrepThreads)
+    k_prep_batch(const __grid_constant__ SlotTable<T> tab, const FrameArgs* fas, const int2* map) {
+    extern __shared__ __align__(16) unsigned char dsm_prep[];
+    const int2 fp = map[blockIdx.x];
+    prep_body<T, K>(tab.prm[fp.x], tab.b[fp.x], fas[fp.x].cur, fp.y, reinterpret_cast<T*>(dsm_prep));
+}
+
 // ---------------------------------------------------------------- (c) likelihood
 // Normaliser ell_{p,m} = logsumexp_j(log w_{j,m}) (+) log(M w0 + kappa)
 // (.cu:1729-1768) and survivor compaction: w_{j,m} = exp(log w - ell) >= min_weight
@@ -539,7 +614,6 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
 // a pair with log w < bpc + log(min_weight) - 1 can never reach min_weight; the first
 // pass remembers the pairs above that bound (up to kLikCand per measurement) and the
 // survivor pass evaluates only those (all pairs again if the list overflowed).
-constexpr int kLikTerms = 12;   // log-constant, PD flag, S^-1 (6), mean (3), pad: 16-byte pieces
 constexpr int kLikCand = 16;   // candidate survivors remembered per measurement
 template <typename T> __host__ __device__ inline size_t likelihood_smem_bytes(int Gcap, int block) {
     return (size_t)Gcap * kLikTerms * sizeof(T) + (size_t)block * kLikCand * sizeof(int);
@@ -565,29 +639,30 @@ __device__ __forceinline__ void load_terms(const double* src, double* t) {
         t[2 * i] = q.x; t[2 * i + 1] = q.y;
     }
 }
+__device__ __forceinline__ void store_terms(float* dst, const float* t) {
+    float4* v = reinterpret_cast<float4*>(dst);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) v[i] = make_float4(t[4 * i], t[4 * i + 1], t[4 * i + 2], t[4 * i + 3]);
+}
+__device__ __forceinline__ void store_terms(double* dst, const double* t) {
+    double2* v = reinterpret_cast<double2*>(dst);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) v[i] = make_double2(t[2 * i], t[2 * i + 1]);
+}
 
 template <typename T, int K>
 __device__ __forceinline__ void likelihood_body(const Params& prm, const Bufs<T>& b, int cur, int M, int p,
                                                 int mblock, T* s_terms) {
     const int m = mblock * blockDim.x + threadIdx.x;
     const int G = min(b.map_n[cur][b.src[p]], prm.Gcap);
-    // per Gaussian: c, pD flag, S^-1, mean, pad; a non-PD posterior's c is staged as -inf
-    // (its weight is LOG0 before the normaliser, kernels.cu:597-598), so that the
-    // normaliser pass needs no test
+    // per Gaussian: c (-inf for a non-PD posterior), pD flag, S^-1, mean, pad -- the
+    // compact rows k_prep wrote, copied into shared memory in 16-byte pieces
     T cm = tneg_inf<T>();
     for (int jj = threadIdx.x; jj < G; jj += blockDim.x) {
-        const T* pr = b.prep + ((size_t)p * prm.Gcap + jj) * kPrep;
-        const T* fr = b.fit + ((size_t)p * prm.Gcap + jj) * kRow;
-        T* t = s_terms + (size_t)jj * kLikTerms;
-        const T c = (pr[0] > tneg_inf<T>() && pr[1] != T(0)) ? pr[0] : tneg_inf<T>();
-        cm = c > cm ? c : cm;
-        t[0] = c;
-        t[1] = pr[1];
-#pragma unroll
-        for (int i = 0; i < 6; ++i) t[2 + i] = pr[kPrepSi + i];
-#pragma unroll
-        for (int a2 = 0; a2 < 3; ++a2) t[8 + a2] = fr[2 + a2];
-        t[11] = T(0);
+        T t[kLikTerms];
+        load_terms(b.lik + ((size_t)p * prm.Gcap + jj) * kLikTerms, t);
+        cm = t[0] > cm ? t[0] : cm;
+        store_terms(s_terms + (size_t)jj * kLikTerms, t);
     }
     T zm[3] = {0, 0, 0};
     if (m < M) {
@@ -790,8 +865,17 @@ template <typename T> struct KalmanView {
     }
 };
 
+// Order of the greedy merge's argmax (and of the map-capacity cut): by weight rounded
+// to single precision, higher first; equal keys by the index tie key.  Exact ties are
+// common (every birth of an unexplained measurement has weight w0 / (M w0 + kappa)), and
+// FP64 weights that differ only in their last bits (a Gaussian term 1e-15 of a
+// normaliser) are ordered differently by any two implementations of the FP64 sums; with
+// single-precision keys both count as ties.  In FP32 mode the key is the weight itself.
+__device__ __forceinline__ float order_key(float w) { return w; }
+__device__ __forceinline__ float order_key(double w) { return __double2float_rn(w); }
 template <typename T> __device__ __forceinline__ bool merge_before(T wa, uint32_t ka, T wb, uint32_t kb) {
-    return wa > wb || (wa == wb && ka < kb);
+    const float fa = order_key(wa), fb = order_key(wb);
+    return fa > fb || (fa == fb && ka < kb);
 }
 
 // Bitonic sort of n_pad (a power of two) items in shared arrays, ordered by
@@ -1135,18 +1219,20 @@ __device__ void merge_members_thread(const View& v, const T* s_w, const int* mem
     row28_store(sparse + (size_t)c * kRow, row);
 }
 
-// Order-preserving integer key of a non-negative weight.
-__device__ __forceinline__ uint64_t weight_key(float w) { return (uint64_t)__float_as_uint(w); }
-__device__ __forceinline__ uint64_t weight_key(double w) { return (uint64_t)__double_as_longlong(w); }
+// Order-preserving integer key of a non-negative weight's order key (the bits of the
+// weight rounded to single precision).
+template <typename T> __device__ __forceinline__ uint64_t weight_key(T w) {
+    return (uint64_t)__float_as_uint(order_key(w));
+}
 
 // Exact k-th largest key among the entries with w >= 0 (k <= their count), by an
-// MSB-first radix select over 8-bit digits.  Block-wide call.
+// MSB-first radix select over the key's four 8-bit digits.  Block-wide call.
 template <typename T>
 __device__ uint64_t select_kth_largest(const T* w, int n, int k) {
     __shared__ int s_hist[256];
     __shared__ uint64_t s_prefix;
     __shared__ int s_k;
-    const int passes = sizeof(T) == 4 ? 4 : 8;
+    const int passes = 4;
     uint64_t prefix = 0, mask = 0;
     if (threadIdx.x == 0) s_k = k;
     for (int d = passes - 1; d >= 0; --d) {

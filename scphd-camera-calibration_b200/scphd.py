@@ -465,7 +465,7 @@ class SCPHDCameraCalibration:
     def set_profiling(self, enable: bool) -> None:
         _check(self._lib.scphd_set_profiling(self._h, int(bool(enable))))
 
-    STAGES = ("predict_parents", "cloud_fit", "likelihood", "merge", "weights", "resample")
+    STAGES = ("predict_parents", "cloud_fit", "likelihood", "merge", "weights", "resample", "kalman_terms")
 
     def stage_times(self):
         """{stage: (total ms, launches)} since the last call (profiling mode)."""

@@ -2,9 +2,10 @@
 
 The reference keeps every merged component and every retained non-detection cloud
 (src/scphdcameracalibration.cu:1923-1942); this implementation bounds each parent's
-map at max_gaussians entries, keeping the largest weights with equal weights in entry
-order and the kept entries in their order.  The device applies the same rule in its
-merge kernel; these CPU tests pin the oracle's statement of it."""
+map at max_gaussians entries, keeping the largest weights -- compared rounded to
+single precision, equal keys in entry order -- and the kept entries in their order.
+The device applies the same rule in its merge kernel; these CPU tests pin the
+oracle's statement of it."""
 import numpy as np
 
 
@@ -22,8 +23,12 @@ def test_cap_keep_rule(orc):
         cap = int(rng.integers(1, n + 1))
         keep = orc.cap_keep(w, cap)
         assert keep.sum() == min(cap, n)
-        expect = sorted(range(n), key=lambda e: (-w[e], e))[:cap]
+        expect = sorted(range(n), key=lambda e: (-np.float32(w[e]), e))[:cap]
         assert np.array_equal(np.flatnonzero(keep), np.sort(expect))
+    # weights equal to single precision are ties: entry order decides
+    w = np.array([0.3, 0.3 * (1 + 1e-12), 0.2, 0.3 * (1 - 1e-12)])
+    assert orc.cap_keep(w, 2).tolist() == [True, True, False, False]
+    assert orc.cap_keep(w, 1).tolist() == [True, False, False, False]
 
 
 def test_capped_map_is_the_cut_of_the_uncapped_map(pkg, orc):
@@ -61,3 +66,20 @@ def test_capped_map_is_the_cut_of_the_uncapped_map(pkg, orc):
             checked += int(sizes_free[p] > cap)
         break
     assert checked > 0, "the cap never bound in this scene"
+
+
+def test_merge_orders_weights_equal_to_single_precision_by_index(orc):
+    """The greedy merge's argmax compares weights rounded to single precision: two
+    components whose FP64 weights differ only in their last bits are a tie, and the
+    reference's index rule (tie key) orders them, whichever is heavier in FP64."""
+    comps = np.zeros((2, 28))
+    comps[0, 0], comps[1, 0] = 0.3, 0.3 * (1 + 1e-12)
+    comps[0, 1:7], comps[1, 1:7] = 0.0, 100.0   # far apart: no merge
+    diag = [0, 2, 5, 9, 14, 20]
+    comps[:, 7 + np.array(diag)] = 1.0
+    out, mem = orc.merge(comps, np.zeros(2, np.uint8), 6.0)
+    assert len(out) == 2 and orc.tie_key(0) < orc.tie_key(1)
+    assert mem.tolist() == [0, 1] and out[0, 0] == comps[0, 0]
+    comps[1, 0] = 0.3 * (1 + 1e-6)   # distinct in single precision: the heavier first
+    out, mem = orc.merge(comps, np.zeros(2, np.uint8), 6.0)
+    assert mem.tolist() == [1, 0]
