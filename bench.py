@@ -238,13 +238,14 @@ def run_b200(args):
     pkg = load_package()
     prec = pkg.SCPHD_FP32 if args.precision == "fp32" else pkg.SCPHD_FP64
     K, W = args.steps, args.warmup
-    n_frames = args.prefill + W + 3 * K + 1
+    n_frames = args.prefill + W + 4 * K + 1
     sc, cfg = pkg.scene.workload(args.workload, precision=prec, filter_index=replica_seed_index(rank),
                                  n_frames=n_frames)
     if args.parents:
         cfg.n_parents = args.parents   # smaller case for profiler captures; not a bench line
     cfg.device = local
     filt = pkg.SCPHDCameraCalibration(cfg)
+    filt.set_fused({"staged": 0, "fused": 1}[args.update_path])
     dev = torch.device("cuda", local)
     dframes = []
     for z in sc.frames:
@@ -289,13 +290,31 @@ def run_b200(args):
     launches = pkg.kernel_launches() - l0
     units = int(c1[6] - c0[6])
     # per-stage device times (events around each stage on the filter's stream)
-    filt.set_profiling(True)
+    filt.set_profiling(True)   # profiling runs the stage kernels one by one, each timed
     c_p0 = filt.counters()
+    prof_meas = 0
     for _ in range(K):
+        prof_meas += int(sc.frames[k].shape[0])
         dstep()
     stages = filt.stage_times()
     filt.set_profiling(False)
     c_p1 = filt.counters()
+    # the fused update's own time (when the tuner chose it): events around each update
+    # (measurement conversion, the fused kernel, the parent-weight kernel)
+    fused_ms = None
+    if shapes.get("fused"):
+        fused_ms = 0.0
+        ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(K):
+            zt = dframes[k]
+            filt.predict(pkg.scene.DT)
+            ea.record(stream)
+            filt.update_device(zt[0].data_ptr(), zt[1].data_ptr(), zt[2].data_ptr(), zt.shape[1], sc.fixed[k])
+            eb.record(stream)
+            filt.resample()
+            eb.synchronize()
+            fused_ms += ea.elapsed_time(eb)
+            k += 1
     # end to end through the host-array C ABI: H2D of the frame, step, D2H of the result
     h2d = d2h = 0
     ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -324,34 +343,60 @@ def run_b200(args):
     value = units_all / (ms_all / 1e3)
     e2e_value = e2e_units_all / (e2e_ms_all / 1e3)
 
-    # roofline of the dominant stage
+    # rooflines.  Algorithmic bytes of each stage over the profiled frames, from the
+    # device counters (Gaussians fitted, clouds read and written, survivors, merged
+    # components): the compulsory reads and writes of the rows each stage consumes and
+    # produces, s bytes per value (4 in FP32).
     peak, peak_kind = read_peaks()
     sz = 4 if prec == pkg.SCPHD_FP32 else 8
     P = int(cfg.particles_per_feature)
-    dom = max(stages.items(), key=lambda kv: kv[1][0])
-    name, (stage_ms, n_launch) = dom
+    N = int(cfg.n_parents)
     fitted = c_p1[10] - c_p0[10]
     rd, wr = c_p1[8] - c_p0[8], c_p1[9] - c_p0[9]
     surv = c_p1[7] - c_p0[7]
     merged = c_p1[11] - c_p0[11]
-    algo_bytes = {
-        # map entry read (28) + fitted row (29) + Kalman terms (47) per Gaussian, clouds read/written
-        "cloud_fit": fitted * (28 + 29 + 47) * sz + (rd + wr) * 7 * P * sz,
-        # Kalman terms + fitted mean read per (parent, Gaussian), survivors written
-        "likelihood": fitted * (8 + 3) * sz * 2 + surv * (4 + sz),
-        # survivors read, merged rows written, new map rows written
-        "merge": surv * (4 + sz) + merged * 28 * sz * 2,
-    }.get(name, 0)
-    per_launch = algo_bytes / max(1, n_launch)
-    avg_ms = stage_ms / max(1, n_launch)
+    ell_vals = N * prof_meas   # normalisers written by the likelihood, read by the merge
+    stage_bytes = {
+        # map entries (merged component: 28 values; carried cloud: weight) read, fitted
+        # rows (29) written, carried clouds read and candidate clouds written (7 P each)
+        "cloud_fit": fitted * (28 + 29) * sz + (rd + wr) * 7 * P * sz,
+        # fitted rows (29) read, Kalman-term rows (48) and likelihood rows (12) written
+        "kalman_terms": fitted * (29 + 48 + 12) * sz,
+        # likelihood rows (12) read, normalisers written, survivors (rank + weight) written
+        "likelihood": fitted * 12 * sz + ell_vals * sz + surv * (4 + sz),
+        # survivors read with their Gaussians' gain, posterior covariance and fitted mean
+        # (18 + 21 + 6); normalisers and fitted weight and pD read; merged rows (28) written
+        # to the merge output and the new map; carried entries written (weight + reference)
+        "merge": surv * (4 + sz + 45 * sz) + ell_vals * sz + fitted * 2 * sz + merged * 28 * sz * 2
+                 + fitted * (sz + 4),
+    }
+    stage_roofline = {}
+    for nm, by in stage_bytes.items():
+        ms, nl = stages.get(nm, (0.0, 0))
+        if nl and ms > 0:
+            gbs = by / nl / (ms / nl / 1e3) / 1e9
+            stage_roofline[nm] = {"bytes_per_launch": by / nl, "ms_per_launch": ms / nl, "achieved_gbs": gbs,
+                                  "frac": gbs / peak}
+    if fused_ms:
+        # one launch per frame covers the four stages of every parent
+        name, n_launch = "fused_update", K
+        per_launch = sum(stage_bytes.values()) / K
+        w_ms = stages.get("weights", (0.0, 1))
+        avg_ms = fused_ms / K - w_ms[0] / max(1, w_ms[1])   # less the parent-weight kernel
+    else:
+        dom = max(((nm, v) for nm, v in stages.items() if nm in stage_bytes), key=lambda kv: kv[1][0])
+        name, (stage_ms, n_launch) = dom
+        per_launch = stage_bytes[name] / max(1, n_launch)
+        avg_ms = stage_ms / max(1, n_launch)
     achieved = per_launch / (avg_ms / 1e3) / 1e9 if avg_ms > 0 else 0.0
     # compute side: algorithmic FP32 flops (about 250 per cloud sample: draw, two
     # camera transforms, prediction, moments) against the nominal FP32 CUDA-core peak
-    # (148 SMs x 128 lanes x 2 flops x 1.965 GHz); the stage is issue-bound, not HBM-bound
+    # (148 SMs x 128 lanes x 2 flops x 1.965 GHz); the cloud fit is issue-bound, not HBM-bound
     fp32_peak_tflops = 148 * 128 * 2 * 1.965e9 / 1e12
-    flops = {"cloud_fit": fitted * P * 250.0}.get(name, 0.0) / max(1, n_launch)
+    flops = fitted * P * 250.0 / max(1, K)
     compute = {"flops_per_launch": flops, "achieved_tflops": flops / (avg_ms / 1e3) / 1e12 if avg_ms > 0 else 0.0,
-               "peak_tflops": fp32_peak_tflops, "peak_source": "nominal FP32 CUDA-core rate"}
+               "peak_tflops": fp32_peak_tflops, "peak_source": "nominal FP32 CUDA-core rate",
+               "flops_counted": "250 per cloud sample (the cloud fit's sampling, transforms, prediction, moments)"}
     compute["frac"] = compute["achieved_tflops"] / fp32_peak_tflops
     traffic = None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
@@ -401,6 +446,7 @@ def run_b200(args):
                      "algorithmic_bytes_per_launch": per_launch, "avg_launch_ms": avg_ms,
                      "compute": compute},
         "stage_ms_per_frame": {k2: v[0] / max(1, v[1]) for k2, v in stages.items()},
+        "stage_roofline": stage_roofline,
         "cpu_baseline": cpu,
         "clocks": clk,
         "counters": {"map_truncations": int(c1[0] - c0[0]), "scratch_overflows": int(c1[1]),
@@ -847,6 +893,8 @@ def main():
     ap.add_argument("--cpu-frames", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the short batched and serving runs")
+    ap.add_argument("--update-path", default="staged", choices=["staged", "fused"],
+                    help="update path of the single filter: one kernel per stage (default) or the fused kernel")
     ap.add_argument("--extra-serve-seconds", type=float, default=20.0, help="serving window of the extra run")
     ap.add_argument("--parents", type=int, default=0, help="override the parent count (profiling only)")
     ap.add_argument("--filters", type=int, default=64, help="filters of the batched_c2 workload")

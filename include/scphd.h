@@ -184,6 +184,20 @@ scphd_status scphd_set_autotune(scphd_filter* f, int32_t enable);
 scphd_status scphd_get_launch_shapes(scphd_filter* f, int32_t* merge_threads, int32_t* likelihood_full,
                                      int32_t* tuned);
 
+/* Update path: 0 (the default) = one kernel per stage; 1 = the fused kernel (one
+ * launch runs the cloud fit, Kalman terms, likelihood and merge of every parent, each
+ * parent's stages in one block, blocks taking parents from a work counter).  The fused
+ * kernel was measured slower than the stage kernels on every workload of this project
+ * (it runs the cloud fit at lower occupancy and each block's Kalman terms as a serial
+ * tail), so it runs only on request.  Per-stage profiling (scphd_set_profiling) always
+ * runs the stage kernels.  Results equal the stage kernels' (FP64: bit for bit; FP32:
+ * to FP32 rounding, as the two builds may contract multiply-adds differently).
+ * scphd_get_fused reports the path the next update takes.  No reference counterpart
+ * (the reference runs its stages as separate kernels and host loops,
+ * src/scphdcameracalibration.cu:1576-2094). */
+scphd_status scphd_set_fused(scphd_filter* f, int32_t mode);
+scphd_status scphd_get_fused(scphd_filter* f, int32_t* fused);
+
 /* The configuration the filter was created with. */
 scphd_status scphd_get_config(scphd_filter* f, scphd_config* out);
 
@@ -247,7 +261,8 @@ scphd_status scphd_device_bytes(const scphd_config* cfg, int64_t* bytes);
 /* ------------------------------------------------------------------ batches
  * Many filters advanced together: every batched step runs predict(dt) + update +
  * resample for all member filters with one kernel launch per stage (seven per frame,
- * whatever the number of filters), each launch covering every filter's parents
+ * or four with the fused update, whatever the number of filters), each launch covering
+ * every filter's parents
  * through a block -> (filter, parent) map.  Member filters must share device,
  * precision and meas_dim; they may differ in size.  While in a batch, the filters
  * issue all their work on the batch's stream (their own stream is restored by
@@ -276,6 +291,12 @@ scphd_status scphd_batch_step(scphd_batch* b, double dt, const scphd_frame* fram
 scphd_status scphd_batch_step_device(scphd_batch* b, double dt, const scphd_frame* frames);
 /* The batch's CUDA stream (a cudaStream_t). */
 void* scphd_batch_stream(scphd_batch* b);
+/* The batch's update path, as scphd_set_fused / scphd_get_fused: 0 (default) the
+ * stage kernels, 1 the fused kernel (set before the first graph capture).  A fused
+ * batch step is four launches per group of up to 32 filters: prediction (with the
+ * frame's measurement conversion), the fused update, parent weights, resampling. */
+scphd_status scphd_batch_set_fused(scphd_batch* b, int32_t mode);
+scphd_status scphd_batch_get_fused(scphd_batch* b, int32_t* fused);
 
 /* ------------------------------------------------------------------ serving
  * A resident request loop over batches.  A job is a filter configuration plus its

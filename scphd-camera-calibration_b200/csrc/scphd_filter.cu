@@ -92,19 +92,28 @@ struct scphd_filter {
     int last_M = 0;
     cudaStream_t own_stream = nullptr;   // the handle's stream while the filter is in a batch
     void* batch = nullptr;               // the batch this filter belongs to, if any
-    // Launch shapes that leave every result unchanged, tuned on the first updates that
-    // have measurements: threads per merge block, and whether the likelihood runs one
-    // block over all of a parent's measurements or 128-thread blocks.  Each shape runs
-    // twice, the likelihood and merge are timed with events, the fastest is kept.
+    // Launch shapes of the stage kernels that leave every result unchanged, tuned on the
+    // first updates that have measurements: threads per merge block, and whether the
+    // likelihood runs one block over all of a parent's measurements or 128-thread blocks.
+    // Each shape runs twice, the update is timed with events, the fastest is kept.
     struct Shape { int merge_threads; int lik_full; };
     static constexpr int kShapes = 4;
     const Shape shapes[kShapes] = {{kMergeThreads, 1}, {128, 1}, {kMergeThreads, 0}, {128, 0}};
+    // The fused update (one launch for the cloud fit, Kalman terms, likelihood and merge
+    // of every parent) runs only on request (scphd_set_fused): measured slower than the
+    // stage kernels on every workload here.
+    int fused_mode = 0;    // 0: stage kernels, 1: fused kernel
+    int fused_grid = 0;    // blocks of the fused kernel (the resident capacity); 0 = unavailable
+    size_t fused_smem = 0;
     bool tuning = true;
     int tune_trials = 0;
     int tune_pending = -1;
     double tune_ms[kShapes] = {0, 0, 0, 0};
     int chosen = 0;
     cudaEvent_t tune_ev[2] = {nullptr, nullptr};
+    // whether the next update takes the fused path (profiling times the stage kernels
+    // one by one)
+    bool fused_next() const { return fused_mode == 1 && !profiling && fused_grid > 0; }
     // the shape for the next update, and whether it is timed
     int pick_shape(bool can_time, bool& timed) {
         timed = tuning && can_time;
@@ -279,6 +288,7 @@ public:
         if (merge_smem > 227 * 1024)
             return fail(SCPHD_ERR_CAPACITY, "max_survivors/max_gaussians need " + std::to_string(merge_smem) +
                                                 " bytes of shared memory per merge block (limit 227 KB)");
+        const void* fused_fn = prm.K == 2 ? (const void*)k_fused<T, 2> : (const void*)k_fused<T, 3>;
         if (prm.K == 2) {
             CUDA_TRY(allow_dynamic_smem((const void*)k_merge<T, 2>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit<T, 2>));
@@ -289,6 +299,16 @@ public:
             CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit<T, 3>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_likelihood<T, 3>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_prep<T, 3>));
+        }
+        fused_smem = fused_smem_bytes<T>(prm.P, prm.Gcap, prm.Scap);
+        fused_grid = 0;
+        if (fused_smem <= 220 * 1024) {   // else the stage kernels only
+            CUDA_TRY(allow_dynamic_smem(fused_fn));
+            int dev = 0, nsm = 0, occ = 0;
+            CUDA_TRY(cudaGetDevice(&dev));
+            CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fused_fn, kFusedThreads, fused_smem));
+            fused_grid = std::min(prm.N, nsm * occ);
         }
         const int N = prm.N;
         k_prior<<<(N + 255) / 256, 256, 0, stream>>>(prm, b.ext, b.lw);
@@ -331,18 +351,6 @@ public:
 
     template <int K> scphd_status update_k(int M, int fixed) {
         const int N = prm.N;
-        CUDA_TRY(cudaMemsetAsync(b.counters + 4, 0, 2 * sizeof(unsigned long long), stream));
-        int h = stage_begin(1);
-        k_cloud_fit<T, K><<<N, 256, fit_smem, stream>>>(prm, b, cur, M, fixed, pending ? 1 : 0, pending_dt, pending_frame,
-                                                  sample_frame[cur], M > 0 ? d_stage : nullptr,
-                                                  M > 0 ? d_stage + M : nullptr, M > 0 ? d_stage + 2 * M : nullptr);
-        LAUNCHED();
-        stage_end(h);
-        h = stage_begin(6);
-        k_prep<T, K><<<N, kPrepThreads, prep_smem_bytes<T>(), stream>>>(prm, b, cur);
-        LAUNCHED();
-        stage_end(h);
-        pending = false;
         {
             const scphd_status ts = tune_collect();
             if (ts != SCPHD_OK) return ts;
@@ -350,23 +358,46 @@ public:
         bool timed = false;
         const Shape sh = shapes[pick_shape(M > 0, timed)];
         if (timed) CUDA_TRY(cudaEventRecord(tune_ev[0], stream));
-        if (M > 0) {
-            const int bs = sh.lik_full ? likelihood_block(M) : 128;
-            dim3 grid(N, (M + bs - 1) / bs);
-            h = stage_begin(2);
-            k_likelihood<T, K><<<grid, bs, likelihood_smem_bytes<T>(prm.Gcap, bs), stream>>>(prm, b, cur, M);
+        if (fused_next()) {
+            k_stage_frame<T, K><<<1, 256, 0, stream>>>(b.z, M > 0 ? d_stage : nullptr, M > 0 ? d_stage + M : nullptr,
+                                                       M > 0 ? d_stage + 2 * M : nullptr, M, b.counters, b.flags + 2);
+            LAUNCHED();
+            const FrameArgs fa{cur, M, fixed, pending ? 1 : 0, pending_dt, pending_frame, sample_frame[cur], frame,
+                               nullptr, nullptr, nullptr};
+            k_fused<T, K><<<fused_grid, kFusedThreads, fused_smem, stream>>>(prm, b, fa, b.flags + 2);
+            LAUNCHED();
+        } else {
+            CUDA_TRY(cudaMemsetAsync(b.counters + 4, 0, 2 * sizeof(unsigned long long), stream));
+            int h = stage_begin(1);
+            k_cloud_fit<T, K><<<N, 256, fit_smem, stream>>>(prm, b, cur, M, fixed, pending ? 1 : 0, pending_dt,
+                                                            pending_frame, sample_frame[cur], M > 0 ? d_stage : nullptr,
+                                                            M > 0 ? d_stage + M : nullptr,
+                                                            M > 0 ? d_stage + 2 * M : nullptr);
+            LAUNCHED();
+            stage_end(h);
+            h = stage_begin(6);
+            k_prep<T, K><<<N, kPrepThreads, prep_smem_bytes<T>(), stream>>>(prm, b, cur);
+            LAUNCHED();
+            stage_end(h);
+            if (M > 0) {
+                const int bs = sh.lik_full ? likelihood_block(M) : 128;
+                dim3 grid(N, (M + bs - 1) / bs);
+                h = stage_begin(2);
+                k_likelihood<T, K><<<grid, bs, likelihood_smem_bytes<T>(prm.Gcap, bs), stream>>>(prm, b, cur, M);
+                LAUNCHED();
+                stage_end(h);
+            }
+            h = stage_begin(3);
+            k_merge<T, K><<<N, sh.merge_threads, merge_smem, stream>>>(prm, b, cur, M, fixed);
             LAUNCHED();
             stage_end(h);
         }
-        h = stage_begin(3);
-        k_merge<T, K><<<N, sh.merge_threads, merge_smem, stream>>>(prm, b, cur, M, fixed);
-        LAUNCHED();
-        stage_end(h);
+        pending = false;
         if (timed) {
             CUDA_TRY(cudaEventRecord(tune_ev[1], stream));
             tune_pending = tune_trials % kShapes;
         }
-        h = stage_begin(4);
+        int h = stage_begin(4);
         k_weights<<<1, 1024, 0, stream>>>(N, b.lw, b.loglik, fixed ? 0 : 1, b.scal, b.counters);
         LAUNCHED();
         stage_end(h);
@@ -869,6 +900,22 @@ scphd_status scphd_get_launch_shapes(scphd_filter* f, int32_t* merge_threads, in
     return SCPHD_OK;
 }
 
+scphd_status scphd_set_fused(scphd_filter* f, int32_t mode) {
+    HANDLE(f);
+    if (mode < 0 || mode > 1) return fail(SCPHD_ERR_INVALID, "mode must be 0 or 1");
+    if (mode == 1 && f->fused_grid <= 0)
+        return fail(SCPHD_ERR_CAPACITY, "the fused kernel needs more shared memory than a block has");
+    f->fused_mode = mode;
+    return SCPHD_OK;
+}
+
+scphd_status scphd_get_fused(scphd_filter* f, int32_t* fused) {
+    HANDLE(f);
+    if (!fused) return fail(SCPHD_ERR_INVALID, "null output");
+    *fused = f->fused_next() ? 1 : 0;
+    return SCPHD_OK;
+}
+
 scphd_status scphd_get_counters(scphd_filter* f, int64_t counters[16]) {
     HANDLE(f);
     if (!counters) return fail(SCPHD_ERR_INVALID, "null output");
@@ -1130,19 +1177,23 @@ struct scphd_batch {
     std::vector<scphd_filter*> fs;
     virtual ~scphd_batch() {}
     virtual scphd_status step(double dt, const scphd_frame* frames, bool device_frames) = 0;
+    virtual scphd_status set_fused(int mode) = 0;
+    virtual int fused_path() const = 0;
 };
 
 namespace {
 
 template <typename T> struct Batch final : scphd_batch {
     // Filters are launched in groups of up to kBatchSlots, each group with its own
-    // parameter table and block maps; seven launches per group and frame.
+    // parameter table and block maps; per group and frame seven launches (one kernel
+    // per stage) or four (prediction, the fused update, weights, resampling).
     struct Group {
         int first = 0, count = 0;       // filters [first, first + count)
         SlotTable<T>* tab = nullptr;    // host copy, passed by value at each launch
         int2* map_parent = nullptr; int n_parent = 0;
         int2* map_pred = nullptr;   int n_pred = 0;
         int4* map_lik = nullptr;    int n_lik = 0;
+        int* work = nullptr;            // the fused update's work counter
     };
     int K = 3;
     bool use_graph = false;
@@ -1160,13 +1211,22 @@ template <typename T> struct Batch final : scphd_batch {
     size_t fit_smem = 0;
     size_t lik_smem = 0;
     int lik_block = 32;
-    // threads per merge block, tuned on the first 4 steps (256 and 128, twice each,
-    // before a graph is captured); results do not depend on it
-    int merge_threads = kMergeThreads;
+    // the update path: the stage kernels with 256 or 128 threads per merge block, tuned
+    // on the first 4 steps before a graph is captured (twice each; results do not depend
+    // on it), or the fused kernel when requested (scphd_batch_set_fused)
+    static constexpr int kPaths = 2;
+    int path = 0;              // 0, 1: stage kernels (merge 256 / 128 threads)
+    int fused_mode = 0;        // 1: the fused kernel instead
+    size_t fused_smem = 0;
+    int fused_grid = 0;        // 0: the fused kernel is unavailable
     bool tuning = true;
     bool capturing = false;
     int tune_trials = 0, tune_pending = -1;
-    double tune_ms[2] = {0, 0};
+    double tune_ms[kPaths] = {0, 0};
+    int path_now() const {     // the path of the step being enqueued (2: fused)
+        if (fused_mode == 1 && fused_grid > 0) return 2;
+        return (tuning && !capturing) ? tune_trials % kPaths : path;
+    }
     cudaEvent_t tune_ev[2] = {nullptr, nullptr};
     void* dev_mem = nullptr;
 
@@ -1224,6 +1284,7 @@ template <typename T> struct Batch final : scphd_batch {
                 stage_total += 3 * (size_t)pr.Mcap;
                 merge_smem = std::max(merge_smem, merge_smem_bytes<T>(pr.Scap, pr.Gcap, kMergeThreads / 32, true));
                 fit_smem = std::max(fit_smem, cloud_fit_smem_bytes<T>(pr.P));
+                fused_smem = std::max(fused_smem, fused_smem_bytes<T>(pr.P, pr.Gcap, pr.Scap));
                 lik_smem = std::max(lik_smem, likelihood_smem_bytes<T>(pr.Gcap, lik_block));
             }
             g.n_parent = (int)mp.back().size();
@@ -1238,6 +1299,7 @@ template <typename T> struct Batch final : scphd_batch {
             probe.take<int2>(mp[gi].size());
             probe.take<int2>(mpred[gi].size());
             probe.take<int4>(ml[gi].size());
+            probe.take<int>(1);
         }
         CUDA_TRY(cudaMalloc(&dev_mem, probe.used));
         Arena a;
@@ -1249,6 +1311,8 @@ template <typename T> struct Batch final : scphd_batch {
             g.map_parent = a.take<int2>(mp[gi].size());
             g.map_pred = a.take<int2>(mpred[gi].size());
             g.map_lik = a.take<int4>(ml[gi].size());
+            g.work = a.take<int>(1);
+            CUDA_TRY(cudaMemset(g.work, 0, sizeof(int)));
             CUDA_TRY(cudaMemcpy(g.map_parent, mp[gi].data(), sizeof(int2) * mp[gi].size(), cudaMemcpyHostToDevice));
             CUDA_TRY(cudaMemcpy(g.map_pred, mpred[gi].data(), sizeof(int2) * mpred[gi].size(), cudaMemcpyHostToDevice));
             CUDA_TRY(cudaMemcpy(g.map_lik, ml[gi].data(), sizeof(int4) * ml[gi].size(), cudaMemcpyHostToDevice));
@@ -1256,6 +1320,18 @@ template <typename T> struct Batch final : scphd_batch {
         CUDA_TRY(cudaMallocHost(&h_fa, sizeof(FrameArgs) * F));
         CUDA_TRY(cudaMallocHost(&h_stage, sizeof(double) * std::max<size_t>(stage_total, 1)));
         if (merge_smem > 227 * 1024) return fail(SCPHD_ERR_CAPACITY, "batch merge needs more than 227 KB of shared memory");
+        {
+            const void* fn = K == 2 ? (const void*)k_fused_batch<T, 2> : (const void*)k_fused_batch<T, 3>;
+            fused_grid = 0;
+            if (fused_smem <= 220 * 1024) {
+                CUDA_TRY(allow_dynamic_smem(fn));
+                int dev = 0, nsm = 0, occ = 0;
+                CUDA_TRY(cudaGetDevice(&dev));
+                CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+                CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kFusedThreads, fused_smem));
+                fused_grid = nsm * occ;
+            }
+        }
         if (K == 2) {
             CUDA_TRY(allow_dynamic_smem((const void*)k_merge_batch<T, 2>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit_batch<T, 2>));
@@ -1279,33 +1355,39 @@ template <typename T> struct Batch final : scphd_batch {
 
     // kernels of one frame, stage by stage over the groups
     template <int KK> scphd_status launch_all() {
-        for (const Group& g : groups) {
-            k_predict_parents_batch<T><<<g.n_pred, 256, 0, stream>>>(*g.tab, d_fa + g.first, g.map_pred);
-            LAUNCHED();
-        }
-        for (const Group& g : groups) {
-            k_cloud_fit_batch<T, KK><<<g.n_parent, 256, fit_smem, stream>>>(*g.tab, d_fa + g.first, g.map_parent);
-            LAUNCHED();
-        }
-        for (const Group& g : groups) {
-            k_prep_batch<T, KK><<<g.n_parent, kPrepThreads, prep_smem_bytes<T>(), stream>>>(*g.tab, d_fa + g.first,
-                                                                                               g.map_parent);
-            LAUNCHED();
-        }
-        for (const Group& g : groups) {
-            k_likelihood_batch<T, KK><<<g.n_lik, lik_block, lik_smem, stream>>>(*g.tab, d_fa + g.first, g.map_lik);
-            LAUNCHED();
-        }
-        const bool timed = tuning && !capturing;
-        const int mt = timed ? (tune_trials % 2 ? 128 : kMergeThreads) : merge_threads;
+        const int pth = path_now();
+        const bool timed = tuning && !capturing && pth < kPaths;
         if (timed) CUDA_TRY(cudaEventRecord(tune_ev[0], stream));
         for (const Group& g : groups) {
-            k_merge_batch<T, KK><<<g.n_parent, mt, merge_smem, stream>>>(*g.tab, d_fa + g.first, g.map_parent);
+            k_predict_parents_batch<T><<<g.n_pred, 256, 0, stream>>>(*g.tab, d_fa + g.first, g.map_pred,
+                                                                     pth == 2 ? g.work : nullptr);
             LAUNCHED();
         }
-        if (timed) {
-            CUDA_TRY(cudaEventRecord(tune_ev[1], stream));
-            tune_pending = tune_trials % 2;
+        if (pth == 2) {
+            for (const Group& g : groups) {
+                k_fused_batch<T, KK><<<std::min(g.n_parent, fused_grid), kFusedThreads, fused_smem, stream>>>(
+                    *g.tab, d_fa + g.first, g.map_parent, g.n_parent, g.work);
+                LAUNCHED();
+            }
+        } else {
+            for (const Group& g : groups) {
+                k_cloud_fit_batch<T, KK><<<g.n_parent, 256, fit_smem, stream>>>(*g.tab, d_fa + g.first, g.map_parent);
+                LAUNCHED();
+            }
+            for (const Group& g : groups) {
+                k_prep_batch<T, KK><<<g.n_parent, kPrepThreads, prep_smem_bytes<T>(), stream>>>(*g.tab, d_fa + g.first,
+                                                                                                   g.map_parent);
+                LAUNCHED();
+            }
+            for (const Group& g : groups) {
+                k_likelihood_batch<T, KK><<<g.n_lik, lik_block, lik_smem, stream>>>(*g.tab, d_fa + g.first, g.map_lik);
+                LAUNCHED();
+            }
+            const int mt = pth == 1 ? 128 : kMergeThreads;
+            for (const Group& g : groups) {
+                k_merge_batch<T, KK><<<g.n_parent, mt, merge_smem, stream>>>(*g.tab, d_fa + g.first, g.map_parent);
+                LAUNCHED();
+            }
         }
         for (const Group& g : groups) {
             k_weights_batch<T><<<g.count, 1024, 0, stream>>>(*g.tab, d_fa + g.first);
@@ -1315,10 +1397,25 @@ template <typename T> struct Batch final : scphd_batch {
             k_resample_batch<T><<<g.count, 1024, 0, stream>>>(*g.tab, d_fa + g.first);
             LAUNCHED();
         }
+        if (timed) {
+            CUDA_TRY(cudaEventRecord(tune_ev[1], stream));
+            tune_pending = tune_trials % kPaths;
+        }
         return SCPHD_OK;
     }
 
-    int launches_per_frame() const { return 7 * (int)groups.size(); }
+    int launches_per_frame() const { return (path_now() == 2 ? 4 : 7) * (int)groups.size(); }
+
+    scphd_status set_fused(int mode) override {
+        if (mode < 0 || mode > 1) return fail(SCPHD_ERR_INVALID, "mode must be 0 or 1");
+        if (mode == 1 && fused_grid <= 0)
+            return fail(SCPHD_ERR_CAPACITY, "the fused kernel needs more shared memory than a block has");
+        if (captured) return fail(SCPHD_ERR_INVALID, "the batch's step graph is already captured");
+        fused_mode = mode;
+        if (mode == 1) tuning = false;   // the stage kernels' merge shape is not needed
+        return SCPHD_OK;
+    }
+    int fused_path() const override { return path_now() == 2 ? 1 : 0; }
 
     scphd_status tune_collect() {
         if (tune_pending < 0) return SCPHD_OK;
@@ -1327,9 +1424,9 @@ template <typename T> struct Batch final : scphd_batch {
         CUDA_TRY(cudaEventElapsedTime(&ms, tune_ev[0], tune_ev[1]));
         tune_ms[tune_pending] += ms;
         tune_pending = -1;
-        if (++tune_trials >= 4) {
+        if (++tune_trials >= 2 * kPaths) {
             tuning = false;
-            merge_threads = tune_ms[1] < tune_ms[0] ? 128 : kMergeThreads;
+            path = tune_ms[1] < tune_ms[0] ? 1 : 0;
         }
         return SCPHD_OK;
     }
@@ -1458,6 +1555,17 @@ scphd_status scphd_batch_create(scphd_filter* const* filters, int32_t n, int32_t
         return s;
     }
     *out = b;
+    return SCPHD_OK;
+}
+
+scphd_status scphd_batch_set_fused(scphd_batch* b, int32_t mode) {
+    if (!b) return fail(SCPHD_ERR_INVALID, "null batch");
+    return b->set_fused(mode);
+}
+
+scphd_status scphd_batch_get_fused(scphd_batch* b, int32_t* fused) {
+    if (!b || !fused) return fail(SCPHD_ERR_INVALID, "null batch or output");
+    *fused = b->fused_path();
     return SCPHD_OK;
 }
 

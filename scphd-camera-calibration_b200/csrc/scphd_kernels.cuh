@@ -1592,19 +1592,27 @@ __device__ __forceinline__ void merge_body(const Params& prm, const Bufs<T>& b, 
             s_r[i] = 0x7fffffff;
         }
     }
-    // parent log-likelihood: sum_m ell + sum_j w_j (.cu:1813-1849), FP64
-    __shared__ double s_red[32];
-    double part = 0;
-    for (int mm = tid; mm < M; mm += blockDim.x) part += (double)b.ell[(size_t)p * prm.Mcap + mm];
-    for (int j = tid; j < G; j += blockDim.x) part += (double)b.fit[((size_t)p * prm.Gcap + j) * kRow];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-    if ((tid & 31) == 0) s_red[tid >> 5] = part;
+    // parent log-likelihood: sum_m ell + sum_j w_j (.cu:1813-1849), FP64, in an order
+    // that does not depend on the block's width (128 or 256 threads, stage kernel or
+    // fused): 256 lane partials, a butterfly within each group of 32, the 8 group
+    // totals in order
+    __shared__ double s_part[256];
+    for (int v = tid; v < 256; v += blockDim.x) {
+        double part = 0;
+        for (int mm = v; mm < M; mm += 256) part += (double)b.ell[(size_t)p * prm.Mcap + mm];
+        for (int j = v; j < G; j += 256) part += (double)b.fit[((size_t)p * prm.Gcap + j) * kRow];
+        s_part[v] = part;
+    }
     __syncthreads();
-    if (tid == 0) {
+    if (tid < 32) {
         double t = 0;
-        for (int w2 = 0; w2 < (int)(blockDim.x >> 5); ++w2) t += s_red[w2];
-        b.loglik[p] = t;
+        for (int grp = 0; grp < 8; ++grp) {
+            double part = s_part[grp * 32 + tid];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+            t += part;
+        }
+        if (tid == 0) b.loglik[p] = t;
     }
     if (sizeof(T) == 4) {
         block_bitonic_sort(PackedSurvItems{s_pk}, n_pad);
@@ -1768,6 +1776,91 @@ __global__ void __launch_bounds__(kMergeThreads, sizeof(T) == 4 ? 3 : 2)
     const int2 fp = map[blockIdx.x];
     const FrameArgs fa = fas[fp.x];
     merge_body<T, K>(tab.prm[fp.x], tab.b[fp.x], fa.cur, fa.M, fa.fixed, fp.y);
+}
+
+// ---------------------------------------------------------------- fused update
+// The update of one parent -- cloud fit, Kalman terms, likelihood and merge -- run by
+// one block, for every parent of a filter (or of a batch group) in one launch: a grid
+// of at most the resident capacity takes parents from a work counter until none is
+// left.  No block waits for another: a parent's stages read only that parent's rows
+// (written to global memory and read back by the same block, from L2), so the grid
+// has no stage boundaries and no per-stage tails.  The launch before converts the
+// measurements and resets the counters; the filter-level weight update and resampling
+// run in the launches after.  Results are those of the stage-by-stage kernels (the
+// same bodies on the same inputs; the likelihood's survivor slots may come in another
+// order, and the merge sorts them).
+constexpr int kFusedThreads = 256;
+template <typename T> inline size_t fused_smem_bytes(int P, int Gcap, int Scap) {
+    size_t s = cloud_fit_smem_bytes<T>(P);
+    const size_t cand[3] = {prep_smem_bytes<T>(), likelihood_smem_bytes<T>(Gcap, kFusedThreads),
+                            merge_smem_bytes<T>(Scap, Gcap, kFusedThreads / 32, true)};
+    for (size_t c : cand) s = c > s ? c : s;
+    return s;
+}
+
+template <typename T, int K>
+__device__ __forceinline__ void fused_parent(const Params& prm, const Bufs<T>& b, const FrameArgs& fa, int p,
+                                             unsigned char* smem) {
+    cloud_fit_body<T, K>(prm, b, fa.cur, fa.M, fa.fixed, fa.has_pred, fa.dt, fa.pred_frame, fa.sample_frame, nullptr,
+                         nullptr, nullptr, p, reinterpret_cast<T*>(smem));
+    __syncthreads();
+    prep_body<T, K>(prm, b, fa.cur, p, reinterpret_cast<T*>(smem));
+    for (int mb = 0; mb * (int)blockDim.x < fa.M; ++mb) {
+        likelihood_body<T, K>(prm, b, fa.cur, fa.M, p, mb, reinterpret_cast<T*>(smem));
+        __syncthreads();
+    }
+    merge_body<T, K>(prm, b, fa.cur, fa.M, fa.fixed, p);
+    __syncthreads();
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kFusedThreads, sizeof(T) == 4 ? 3 : 2)
+    k_fused(__grid_constant__ const Params prm, __grid_constant__ const Bufs<T> b, const FrameArgs fa, int* work) {
+    extern __shared__ __align__(16) unsigned char dsm_fused[];
+    __shared__ int s_item;
+    while (true) {
+        if (threadIdx.x == 0) s_item = atomicAdd(work, 1);
+        __syncthreads();
+        const int p = s_item;
+        __syncthreads();
+        if (p >= prm.N) break;
+        fused_parent<T, K>(prm, b, fa, p, dsm_fused);
+    }
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kFusedThreads, sizeof(T) == 4 ? 3 : 2)
+    k_fused_batch(const __grid_constant__ SlotTable<T> tab, const FrameArgs* fas, const int2* map, int n_items,
+                  int* work) {
+    extern __shared__ __align__(16) unsigned char dsm_fused[];
+    __shared__ int s_item;
+    while (true) {
+        if (threadIdx.x == 0) s_item = atomicAdd(work, 1);
+        __syncthreads();
+        const int it = s_item;
+        __syncthreads();
+        if (it >= n_items) break;
+        const int2 fp = map[it];
+        const FrameArgs fa = fas[fp.x];
+        fused_parent<T, K>(tab.prm[fp.x], tab.b[fp.x], fa, fp.y, dsm_fused);
+    }
+}
+
+// The launch before a single filter's fused update: this frame's measurements into the
+// T layout (u, v, d), the per-update counters and the work counter to 0.
+template <typename T, int K>
+__global__ void k_stage_frame(T* z, const double* zu, const double* zv, const double* zd, int M,
+                              unsigned long long* counters, int* work) {
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+        z[m * 3 + 0] = (T)zu[m];
+        z[m * 3 + 1] = (T)zv[m];
+        z[m * 3 + 2] = (K == 3 && zd) ? (T)zd[m] : T(0);
+    }
+    if (threadIdx.x == 0) {
+        counters[4] = 0;
+        counters[5] = 0;
+        *work = 0;
+    }
 }
 
 // ---------------------------------------------------------------- parent weights
@@ -1974,16 +2067,32 @@ __global__ void __launch_bounds__(1024) k_resample_batch(const __grid_constant__
                   fas[f].frame, 0, -1.0, b.counters);
 }
 
-// map entry: (filter, first parent of a 256-parent block)
+// map entry: (filter, first parent of a 256-parent block).  The first block of each
+// filter also resets its per-update counters and converts its frame's measurements
+// into the T layout (u, v, d) for the fused update; block 0 resets the group's work
+// counter (may be null).
 template <typename T>
-__global__ void k_predict_parents_batch(const __grid_constant__ SlotTable<T> tab, const FrameArgs* fas, const int2* map) {
+__global__ void k_predict_parents_batch(const __grid_constant__ SlotTable<T> tab, const FrameArgs* fas, const int2* map,
+                                        int* work) {
     const int2 fp = map[blockIdx.x];
     const Bufs<T>& b = tab.b[fp.x];
-    if (fp.y == 0 && threadIdx.x == 0) {   // counters of "the last update" start at 0
-        b.counters[4] = 0;
-        b.counters[5] = 0;
+    const FrameArgs& fa = fas[fp.x];
+    if (fp.y == 0) {
+        if (threadIdx.x == 0) {   // counters of "the last update" start at 0
+            b.counters[4] = 0;
+            b.counters[5] = 0;
+        }
+        if (fa.zu != nullptr) {
+            const int K = tab.prm[fp.x].K;
+            for (int m = threadIdx.x; m < fa.M; m += blockDim.x) {
+                b.z[m * 3 + 0] = (T)fa.zu[m];
+                b.z[m * 3 + 1] = (T)fa.zv[m];
+                b.z[m * 3 + 2] = (K == 3 && fa.zd) ? (T)fa.zd[m] : T(0);
+            }
+        }
     }
-    predict_parents_body(tab.prm[fp.x], b.ext, fas[fp.x].dt, fas[fp.x].frame, fp.y + threadIdx.x);
+    if (work != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *work = 0;
+    predict_parents_body(tab.prm[fp.x], b.ext, fa.dt, fa.frame, fp.y + threadIdx.x);
 }
 
 // ---------------------------------------------------------------- cloud materialisation

@@ -204,6 +204,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "scphd_get_config": (i32, [vp, P(ScphdConfig)]),
         "scphd_set_autotune": (i32, [vp, i32]),
         "scphd_get_launch_shapes": (i32, [vp, P(i32), P(i32), P(i32)]),
+        "scphd_set_fused": (i32, [vp, i32]),
+        "scphd_get_fused": (i32, [vp, P(i32)]),
+        "scphd_batch_set_fused": (i32, [vp, i32]),
+        "scphd_batch_get_fused": (i32, [vp, P(i32)]),
         "scphd_config_from_file": (i32, [ctypes.c_char_p, P(ScphdConfig), P(ScphdRunOptions)]),
         "scphd_read_mat_frames": (i32, [ctypes.c_char_p, ctypes.c_char_p, P(i32), P(i32), P(i32), P(d), i64]),
         "scphd_write_mat": (i32, [vp, ctypes.c_char_p, i32]),
@@ -385,7 +389,14 @@ class SCPHDCameraCalibration:
     def launch_shapes(self) -> dict:
         mt, lf, tuned = ctypes.c_int32(0), ctypes.c_int32(0), ctypes.c_int32(0)
         _check(self._lib.scphd_get_launch_shapes(self._h, ctypes.byref(mt), ctypes.byref(lf), ctypes.byref(tuned)))
-        return {"merge_threads": mt.value, "likelihood_full": bool(lf.value), "tuned": bool(tuned.value)}
+        fz = ctypes.c_int32(0)
+        _check(self._lib.scphd_get_fused(self._h, ctypes.byref(fz)))
+        return {"merge_threads": mt.value, "likelihood_full": bool(lf.value), "tuned": bool(tuned.value),
+                "fused": bool(fz.value)}
+
+    def set_fused(self, mode: int) -> None:
+        """Update path: 0 one kernel per stage (default), 1 the fused kernel."""
+        _check(self._lib.scphd_set_fused(self._h, int(mode)))
 
     def writeMat(self, path: str, save_all_maps: bool = False) -> None:
         """The reference's writeMat: particles, weights and the MAP parent's map (and
@@ -545,6 +556,15 @@ class SCPHDBatch:
 
     def stream_handle(self) -> int:
         return int(self._lib.scphd_batch_stream(self._h) or 0)
+
+    def set_fused(self, mode: int) -> None:
+        """Update path before the first graph capture: 0 stage kernels (default), 1 fused."""
+        _check(self._lib.scphd_batch_set_fused(self._h, int(mode)))
+
+    def fused(self) -> bool:
+        fz = ctypes.c_int32(0)
+        _check(self._lib.scphd_batch_get_fused(self._h, ctypes.byref(fz)))
+        return bool(fz.value)
 
     def synchronize(self) -> None:
         for f in self.filters:

@@ -18,7 +18,7 @@ def test_tuned_shapes_leave_results_unchanged(pkg, precision):
                                   precision=precision, calib=sc.calib, seed=61, particles_per_feature=40)
     tuned, plain = pkg.SCPHDCameraCalibration(cfg), pkg.SCPHDCameraCalibration(cfg)
     plain.set_autotune(False)
-    assert plain.launch_shapes() == {"merge_threads": 256, "likelihood_full": True, "tuned": True}
+    assert plain.launch_shapes() == {"merge_threads": 256, "likelihood_full": True, "tuned": True, "fused": False}
     assert not tuned.launch_shapes()["tuned"]
     for k, z in enumerate(sc.frames):
         for f in (tuned, plain):
@@ -31,3 +31,47 @@ def test_tuned_shapes_leave_results_unchanged(pkg, precision):
             assert np.array_equal(tuned.mixture(1, p), plain.mixture(1, p)), f"frame {k} parent {p}"
     s = tuned.launch_shapes()
     assert s["tuned"] and s["merge_threads"] in (128, 256)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_fused_update_equals_stage_kernels(pkg, precision):
+    """The fused update (one launch: cloud fit, Kalman terms, likelihood and merge of
+    every parent) and the stage kernels give the same states, maps and mixtures -- in
+    FP64 bit for bit; in FP32 to FP32 rounding on the first frames (the two builds may
+    contract multiply-adds differently, and later frames then part at thresholds) --
+    on a scene whose maps reach the capacity and with more measurements than a fused
+    block has threads (two likelihood passes per parent)."""
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    sc = pkg.scene.make_scene(n_landmarks=420, n_frames=8, clutter_rate=90.0, seed=pkg.scene.scene_seed(6, 1))
+    cfg = pkg.scene.filter_config(n_parents=72, max_gaussians=96, max_meas=384, clutter_rate=90.0,
+                                  precision=precision, calib=sc.calib, seed=62, particles_per_feature=50)
+    fused, staged = pkg.SCPHDCameraCalibration(cfg), pkg.SCPHDCameraCalibration(cfg)
+    fused.set_fused(1)
+    staged.set_fused(0)
+    assert fused.launch_shapes()["fused"] and not staged.launch_shapes()["fused"]
+    exact = precision == 1
+    same = (lambda a, b: np.array_equal(a, b)) if exact else \
+        (lambda a, b: a.shape == b.shape and np.allclose(a, b, rtol=1e-4, atol=1e-6))
+    big = False
+    n_frames = len(sc.frames) if exact else 3
+    for k, z in enumerate(sc.frames[:n_frames]):
+        big |= z.shape[0] > 256
+        for f in (fused, staged):
+            f.step(pkg.scene.DT, z[:, 0], z[:, 1], fixed_camera=sc.fixed[k], d=z[:, 2])
+        st_a, lw_a = fused.particles()
+        st_b, lw_b = staged.particles()
+        assert same(st_a, st_b) and same(lw_a, lw_b), f"frame {k}"
+        assert np.array_equal(fused.map_sizes(), staged.map_sizes()), f"frame {k} map sizes"
+        for p in range(0, cfg.n_parents, 5):
+            assert same(fused.mixture(1, p), staged.mixture(1, p)), f"frame {k} parent {p} merged"
+            assert same(fused.mixture(0, p), staged.mixture(0, p)), f"frame {k} parent {p} fitted"
+            assert same(fused.map_weights(p), staged.map_weights(p)), f"frame {k} parent {p} map"
+        e_a, l_a = fused.normalizers(z.shape[0])
+        e_b, l_b = staged.normalizers(z.shape[0])
+        assert same(e_a, e_b) and same(l_a, l_b), f"frame {k} normalisers"
+    assert big, "no frame had more measurements than a fused block's threads"
+    if exact:
+        assert np.array_equal(fused.counters()[[0, 2, 3, 4, 5, 6, 7, 11]],
+                              staged.counters()[[0, 2, 3, 4, 5, 6, 7, 11]])
+        assert fused.counters()[0] > 0, "the map capacity never bound"
