@@ -292,11 +292,13 @@ public:
         if (prm.K == 2) {
             CUDA_TRY(allow_dynamic_smem((const void*)k_merge<T, 2>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit<T, 2>));
+            CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit<T, 2, kFitP>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_likelihood<T, 2>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_prep<T, 2>));
         } else {
             CUDA_TRY(allow_dynamic_smem((const void*)k_merge<T, 3>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit<T, 3>));
+            CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit<T, 3, kFitP>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_likelihood<T, 3>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_prep<T, 3>));
         }
@@ -369,10 +371,15 @@ public:
         } else {
             CUDA_TRY(cudaMemsetAsync(b.counters + 4, 0, 2 * sizeof(unsigned long long), stream));
             int h = stage_begin(1);
-            k_cloud_fit<T, K><<<N, 256, fit_smem, stream>>>(prm, b, cur, M, fixed, pending ? 1 : 0, pending_dt,
-                                                            pending_frame, sample_frame[cur], M > 0 ? d_stage : nullptr,
-                                                            M > 0 ? d_stage + M : nullptr,
-                                                            M > 0 ? d_stage + 2 * M : nullptr);
+            const double* zs[3] = {M > 0 ? d_stage : nullptr, M > 0 ? d_stage + M : nullptr,
+                                   M > 0 ? d_stage + 2 * M : nullptr};
+            if (fit_specialised<T>(prm))
+                k_cloud_fit<T, K, kFitP><<<N, 256, fit_smem, stream>>>(prm, b, cur, M, fixed, pending ? 1 : 0,
+                                                                       pending_dt, pending_frame, sample_frame[cur],
+                                                                       zs[0], zs[1], zs[2]);
+            else
+                k_cloud_fit<T, K><<<N, 256, fit_smem, stream>>>(prm, b, cur, M, fixed, pending ? 1 : 0, pending_dt,
+                                                                pending_frame, sample_frame[cur], zs[0], zs[1], zs[2]);
             LAUNCHED();
             stage_end(h);
             h = stage_begin(6);
@@ -627,7 +634,8 @@ Params make_params(const scphd_config& c) {
     p.Mcap = c.max_measurements;
     p.Scap = c.max_survivors > 0 ? c.max_survivors : 4 * c.max_gaussians + c.max_measurements;
     p.K = c.meas_dim;
-    p.Ps = round_up(c.particles_per_feature, c.precision == SCPHD_FP64 ? 4 : 8);
+    p.Ps = c.precision == SCPHD_FP64 ? cloud_stride<double>(c.particles_per_feature)
+                                     : cloud_stride<float>(c.particles_per_feature);
     p.model.fx = c.fx; p.model.fy = c.fy; p.model.u0 = c.u0; p.model.v0 = c.v0;
     p.model.B = c.baseline; p.model.pd = c.pd;
     p.model.var[0] = c.std_u * c.std_u;
@@ -1194,6 +1202,7 @@ template <typename T> struct Batch final : scphd_batch {
         int2* map_pred = nullptr;   int n_pred = 0;
         int4* map_lik = nullptr;    int n_lik = 0;
         int* work = nullptr;            // the fused update's work counter
+        bool fit_p = false;             // every member has kFitP samples per feature
     };
     int K = 3;
     bool use_graph = false;
@@ -1267,6 +1276,7 @@ template <typename T> struct Batch final : scphd_batch {
             g.first = first;
             g.count = std::min(kBatchSlots, F - first);
             g.tab = new SlotTable<T>();
+            g.fit_p = true;
             mp.emplace_back();
             mpred.emplace_back();
             ml.emplace_back();
@@ -1274,6 +1284,7 @@ template <typename T> struct Batch final : scphd_batch {
                 const Filter<T>* fl = filt(first + i);
                 const Params& pr = fl->prm;
                 g.tab->prm[i] = pr;
+                g.fit_p = g.fit_p && fit_specialised<T>(pr);
                 g.tab->b[i] = fl->b;
                 for (int q = 0; q < pr.N; ++q) mp.back().push_back(make_int2(i, q));
                 for (int q = 0; q < pr.N; q += 256) mpred.back().push_back(make_int2(i, q));
@@ -1335,11 +1346,13 @@ template <typename T> struct Batch final : scphd_batch {
         if (K == 2) {
             CUDA_TRY(allow_dynamic_smem((const void*)k_merge_batch<T, 2>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit_batch<T, 2>));
+            CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit_batch<T, 2, kFitP>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_likelihood_batch<T, 2>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_prep_batch<T, 2>));
         } else {
             CUDA_TRY(allow_dynamic_smem((const void*)k_merge_batch<T, 3>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit_batch<T, 3>));
+            CUDA_TRY(allow_dynamic_smem((const void*)k_cloud_fit_batch<T, 3, kFitP>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_likelihood_batch<T, 3>));
             CUDA_TRY(allow_dynamic_smem((const void*)k_prep_batch<T, 3>));
         }
@@ -1371,7 +1384,12 @@ template <typename T> struct Batch final : scphd_batch {
             }
         } else {
             for (const Group& g : groups) {
-                k_cloud_fit_batch<T, KK><<<g.n_parent, 256, fit_smem, stream>>>(*g.tab, d_fa + g.first, g.map_parent);
+                if (g.fit_p)
+                    k_cloud_fit_batch<T, KK, kFitP><<<g.n_parent, 256, fit_smem, stream>>>(*g.tab, d_fa + g.first,
+                                                                                           g.map_parent);
+                else
+                    k_cloud_fit_batch<T, KK><<<g.n_parent, 256, fit_smem, stream>>>(*g.tab, d_fa + g.first,
+                                                                                    g.map_parent);
                 LAUNCHED();
             }
             for (const Group& g : groups) {

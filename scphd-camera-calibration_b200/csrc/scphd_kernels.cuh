@@ -232,9 +232,12 @@ __device__ __forceinline__ double moment_sweep(const double* a, const double* b,
 // banks apart, so that the eight rows a lane-per-moment sweep reads at one sample
 // index (16-byte pieces) fall in distinct banks; the second Gaussian's rows start 16
 // values further on, so that the two half-warps' stores of one row never share a bank.
-template <typename T> __host__ __device__ inline int stage_stride(int P4) {
-    if (sizeof(T) == 4) return (P4 % 8 == 4) ? P4 : P4 + 4;
-    return P4 + 2;
+template <typename T> __host__ __device__ constexpr int stage_stride(int P4) {
+    return sizeof(T) == 4 ? ((P4 % 8 == 4) ? P4 : P4 + 4) : P4 + 2;
+}
+// stride of a cloud's rows (x, y, z, vx, vy, vz, weight): P rounded up to 32 bytes
+template <typename T> __host__ __device__ constexpr int cloud_stride(int P) {
+    return sizeof(T) == 4 ? ((P + 7) & ~7) : ((P + 3) & ~3);
 }
 constexpr int kFitWarps = 8;
 constexpr int kStageRows = 8;   // r d[6], r, w'
@@ -243,7 +246,15 @@ template <typename T> __host__ __device__ inline size_t cloud_fit_smem_bytes(int
     return (size_t)kFitWarps * 2 * (kStageRows * stage_stride<T>(P4) + 16) * sizeof(T);   // sample rows
 }
 
-template <typename T, int K>
+// PC > 0: the body for exactly PC samples per feature, whose strides and loop bounds are
+// compile-time constants (immediate address offsets instead of per-sample index
+// arithmetic); PC == 0: any P.  kFitP is the specialised count (the configurations'
+// particles_per_feature); fit_specialised says whether a filter's parameters match it.
+constexpr int kFitP = 100;
+template <typename T> __host__ __device__ inline bool fit_specialised(const Params& prm) {
+    return prm.P == kFitP && prm.Ps == cloud_stride<T>(kFitP);
+}
+template <typename T, int K, int PC = 0>
 __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>& b, int cur, int M, int fixed,
                                                int has_pred, double dt, uint32_t pred_frame, uint32_t sample_frame,
                                                const double* zu, const double* zv, const double* zd, int p,
@@ -258,7 +269,7 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int row = b.src[p];
     const int G = min(b.map_n[cur][row], prm.Gcap);
-    const int P = prm.P, Ps = prm.Ps;
+    const int P = PC > 0 ? PC : prm.P, Ps = PC > 0 ? cloud_stride<T>(PC) : prm.Ps;
     const int P4 = (P + 3) & ~3;
     const int sY = stage_stride<T>(P4);
     T* Ywarp = s_stage + (size_t)warp * 2 * (kStageRows * sY + 16);   // per Gaussian of the pair: r d[6], r, w'
@@ -496,23 +507,23 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
 }
 
 
-template <typename T, int K>
+template <typename T, int K, int PC = 0>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
     k_cloud_fit(__grid_constant__ const Params prm, __grid_constant__ const Bufs<T> b, int cur, int M, int fixed,
                 int has_pred, double dt, uint32_t pred_frame, uint32_t sample_frame, const double* zu,
                 const double* zv, const double* zd) {
     extern __shared__ __align__(16) unsigned char dsm_fit[];
-    cloud_fit_body<T, K>(prm, b, cur, M, fixed, has_pred, dt, pred_frame, sample_frame, zu, zv, zd, blockIdx.x,
+    cloud_fit_body<T, K, PC>(prm, b, cur, M, fixed, has_pred, dt, pred_frame, sample_frame, zu, zv, zd, blockIdx.x,
                          reinterpret_cast<T*>(dsm_fit));
 }
 
-template <typename T, int K>
+template <typename T, int K, int PC = 0>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
     k_cloud_fit_batch(const __grid_constant__ SlotTable<T> tab, const FrameArgs* fas, const int2* map) {
     extern __shared__ __align__(16) unsigned char dsm_fit[];
     const int2 fp = map[blockIdx.x];
     const FrameArgs fa = fas[fp.x];
-    cloud_fit_body<T, K>(tab.prm[fp.x], tab.b[fp.x], fa.cur, fa.M, fa.fixed, fa.has_pred, fa.dt, fa.pred_frame,
+    cloud_fit_body<T, K, PC>(tab.prm[fp.x], tab.b[fp.x], fa.cur, fa.M, fa.fixed, fa.has_pred, fa.dt, fa.pred_frame,
                          fa.sample_frame, fa.zu, fa.zv, fa.zd, fp.y, reinterpret_cast<T*>(dsm_fit));
 }
 
