@@ -50,7 +50,7 @@ enum { SCPHD_FP32 = 0, SCPHD_FP64 = 1 };
  * precision and seed are additions of this implementation. */
 typedef struct scphd_config {
     int32_t n_parents;              /* n_particles */
-    int32_t particles_per_feature;  /* Monte-Carlo samples per daughter Gaussian, <= 256 (<= 216 in FP64) */
+    int32_t particles_per_feature;  /* Monte-Carlo samples per daughter Gaussian, <= 256 */
     int32_t max_gaussians;          /* per-parent map capacity (G_max) */
     int32_t max_measurements;       /* per-frame measurement capacity (M_max) */
     int32_t meas_dim;               /* 2: (u,v) as the reference; 3: (u,v,d) */
@@ -198,6 +198,18 @@ scphd_status scphd_get_launch_shapes(scphd_filter* f, int32_t* merge_threads, in
 scphd_status scphd_set_fused(scphd_filter* f, int32_t mode);
 scphd_status scphd_get_fused(scphd_filter* f, int32_t* fused);
 
+/* Cloud-fit tiling: blocks per parent (1, 2 or 4).  Each block has 8 warps and the
+ * parent's daughter Gaussians are dealt out over the warps of all its blocks (a warp
+ * per Gaussian), so 2 or 4 blocks per parent fill the GPU when a filter has few
+ * parents (256 blocks leave most of 148 SMs x 4 block slots idle).  By default the
+ * first updates with measurements time the cloud-fit launch at each split (twice) and
+ * keep the fastest; scphd_set_fit_split fixes one (and ends that tuning),
+ * scphd_set_autotune(f, 0) fixes 1.  Results do not depend on the split.  *tuned = 1
+ * once a choice is made.  No reference counterpart (fitGaussiansKernel runs a block
+ * per Gaussian, src/kernels.cu:102-438). */
+scphd_status scphd_set_fit_split(scphd_filter* f, int32_t blocks_per_parent);
+scphd_status scphd_get_fit_split(scphd_filter* f, int32_t* blocks_per_parent, int32_t* tuned);
+
 /* The configuration the filter was created with. */
 scphd_status scphd_get_config(scphd_filter* f, scphd_config* out);
 
@@ -297,6 +309,11 @@ void* scphd_batch_stream(scphd_batch* b);
  * frame's measurement conversion), the fused update, parent weights, resampling. */
 scphd_status scphd_batch_set_fused(scphd_batch* b, int32_t mode);
 scphd_status scphd_batch_get_fused(scphd_batch* b, int32_t* fused);
+/* The batch's cloud-fit tiling, as scphd_set_fit_split / scphd_get_fit_split (one
+ * split for all member filters, tuned on the batch's first six steps before its graph
+ * is captured; set it before the capture). */
+scphd_status scphd_batch_set_fit_split(scphd_batch* b, int32_t blocks_per_parent);
+scphd_status scphd_batch_get_fit_split(scphd_batch* b, int32_t* blocks_per_parent, int32_t* tuned);
 
 /* ------------------------------------------------------------------ serving
  * A resident request loop over batches.  A job is a filter configuration plus its

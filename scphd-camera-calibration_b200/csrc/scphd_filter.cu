@@ -111,6 +111,16 @@ struct scphd_filter {
     double tune_ms[kShapes] = {0, 0, 0, 0};
     int chosen = 0;
     cudaEvent_t tune_ev[2] = {nullptr, nullptr};
+    // Blocks per parent of the cloud fit (the parent's Gaussians dealt out over the warps
+    // of all its blocks): 1, 2 or 4, tuned on the same first updates by the cloud-fit
+    // launch's own event time (each twice), or fixed by scphd_set_fit_split.  Every
+    // split computes the same values.
+    static constexpr int kFitSplits = 3;
+    const int fit_splits[kFitSplits] = {1, 2, 4};
+    bool fit_tuning = true;
+    int fit_trials = 0, fit_pending = -1, fit_chosen = 0;
+    double fit_ms[kFitSplits] = {0, 0, 0};
+    cudaEvent_t fit_ev[2] = {nullptr, nullptr};
     // whether the next update takes the fused path (profiling times the stage kernels
     // one by one)
     bool fused_next() const { return fused_mode == 1 && !profiling && fused_grid > 0; }
@@ -121,6 +131,18 @@ struct scphd_filter {
     }
     // fold in the last timed update (waits for it)
     scphd_status tune_collect() {
+        if (fit_pending >= 0) {
+            CUDA_TRY(cudaEventSynchronize(fit_ev[1]));
+            float ms = 0;
+            CUDA_TRY(cudaEventElapsedTime(&ms, fit_ev[0], fit_ev[1]));
+            fit_ms[fit_pending] += ms;
+            fit_pending = -1;
+            if (++fit_trials >= 2 * kFitSplits) {
+                fit_tuning = false;
+                for (int k = 1; k < kFitSplits; ++k)
+                    if (fit_ms[k] < fit_ms[fit_chosen]) fit_chosen = k;
+            }
+        }
         if (tune_pending < 0) return SCPHD_OK;
         CUDA_TRY(cudaEventSynchronize(tune_ev[1]));
         float ms = 0;
@@ -178,6 +200,8 @@ struct scphd_filter {
     virtual ~scphd_filter() {
         for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
         for (cudaEvent_t e : tune_ev)
+            if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : fit_ev)
             if (e) cudaEventDestroy(e);
     }
     virtual scphd_status init() = 0;
@@ -265,6 +289,8 @@ public:
         CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         CUDA_TRY(cudaEventCreate(&tune_ev[0]));
         CUDA_TRY(cudaEventCreate(&tune_ev[1]));
+        CUDA_TRY(cudaEventCreate(&fit_ev[0]));
+        CUDA_TRY(cudaEventCreate(&fit_ev[1]));
         CUDA_TRY(cudaEventCreateWithFlags(&stage_ev, cudaEventDisableTiming));
         CUDA_TRY(cudaMallocHost(&h_stage, sizeof(double) * 3 * prm.Mcap));
         Arena probe;
@@ -282,9 +308,11 @@ public:
         CUDA_TRY(cudaMemsetAsync(p, 0, probe.used, stream));
         merge_smem = merge_smem_bytes<T>(prm.Scap, prm.Gcap, kMergeThreads / 32, true);
         fit_smem = cloud_fit_smem_bytes<T>(prm.P);
-        if (fit_smem > 220 * 1024)   // with the kernel's static shared memory, within 227 KB per block
+        // with the kernel's static shared memory (20 KB at most), within 227 KB per block:
+        // every particles_per_feature up to 256 fits (FP64 at 256: 147 KB of sample rows)
+        if (fit_smem > 200 * 1024)
             return fail(SCPHD_ERR_CAPACITY, "particles_per_feature needs " + std::to_string(fit_smem) +
-                                                " bytes of shared memory per cloud-fit block (FP64 allows up to 216)");
+                                                " bytes of shared memory per cloud-fit block (limit 200 KB)");
         if (merge_smem > 227 * 1024)
             return fail(SCPHD_ERR_CAPACITY, "max_survivors/max_gaussians need " + std::to_string(merge_smem) +
                                                 " bytes of shared memory per merge block (limit 227 KB)");
@@ -373,14 +401,22 @@ public:
             int h = stage_begin(1);
             const double* zs[3] = {M > 0 ? d_stage : nullptr, M > 0 ? d_stage + M : nullptr,
                                    M > 0 ? d_stage + 2 * M : nullptr};
+            const bool fit_timed = fit_tuning && M > 0;
+            const int fs = fit_timed ? fit_trials % kFitSplits : fit_chosen, split = fit_splits[fs];
+            if (fit_timed) CUDA_TRY(cudaEventRecord(fit_ev[0], stream));
             if (fit_specialised<T>(prm))
-                k_cloud_fit<T, K, kFitP><<<N, 256, fit_smem, stream>>>(prm, b, cur, M, fixed, pending ? 1 : 0,
-                                                                       pending_dt, pending_frame, sample_frame[cur],
-                                                                       zs[0], zs[1], zs[2]);
+                k_cloud_fit<T, K, kFitP><<<N * split, 256, fit_smem, stream>>>(
+                    prm, b, cur, M, fixed, pending ? 1 : 0, pending_dt, pending_frame, sample_frame[cur], zs[0], zs[1],
+                    zs[2], split);
             else
-                k_cloud_fit<T, K><<<N, 256, fit_smem, stream>>>(prm, b, cur, M, fixed, pending ? 1 : 0, pending_dt,
-                                                                pending_frame, sample_frame[cur], zs[0], zs[1], zs[2]);
+                k_cloud_fit<T, K><<<N * split, 256, fit_smem, stream>>>(prm, b, cur, M, fixed, pending ? 1 : 0,
+                                                                        pending_dt, pending_frame, sample_frame[cur],
+                                                                        zs[0], zs[1], zs[2], split);
             LAUNCHED();
+            if (fit_timed) {
+                CUDA_TRY(cudaEventRecord(fit_ev[1], stream));
+                fit_pending = fs;
+            }
             stage_end(h);
             h = stage_begin(6);
             k_prep<T, K><<<N, kPrepThreads, prep_smem_bytes<T>(), stream>>>(prm, b, cur);
@@ -894,7 +930,29 @@ scphd_status scphd_set_autotune(scphd_filter* f, int32_t enable) {
         f->tuning = false;
         f->tune_pending = -1;
         f->chosen = 0;
+        f->fit_tuning = false;
+        f->fit_pending = -1;
+        f->fit_chosen = 0;
     }
+    return SCPHD_OK;
+}
+
+scphd_status scphd_set_fit_split(scphd_filter* f, int32_t blocks_per_parent) {
+    if (!f) return fail(SCPHD_ERR_INVALID, "null handle");
+    for (int k = 0; k < scphd_filter::kFitSplits; ++k)
+        if (f->fit_splits[k] == blocks_per_parent) {
+            f->fit_tuning = false;
+            f->fit_pending = -1;
+            f->fit_chosen = k;
+            return SCPHD_OK;
+        }
+    return fail(SCPHD_ERR_INVALID, "blocks_per_parent must be 1, 2 or 4");
+}
+
+scphd_status scphd_get_fit_split(scphd_filter* f, int32_t* blocks_per_parent, int32_t* tuned) {
+    if (!f) return fail(SCPHD_ERR_INVALID, "null handle");
+    if (blocks_per_parent) *blocks_per_parent = f->fit_splits[f->fit_chosen];
+    if (tuned) *tuned = f->fit_tuning ? 0 : 1;
     return SCPHD_OK;
 }
 
@@ -1187,6 +1245,8 @@ struct scphd_batch {
     virtual scphd_status step(double dt, const scphd_frame* frames, bool device_frames) = 0;
     virtual scphd_status set_fused(int mode) = 0;
     virtual int fused_path() const = 0;
+    virtual scphd_status set_fit_split(int blocks_per_parent) = 0;
+    virtual void get_fit_split(int32_t* blocks_per_parent, int32_t* tuned) const = 0;
 };
 
 namespace {
@@ -1237,11 +1297,21 @@ template <typename T> struct Batch final : scphd_batch {
         return (tuning && !capturing) ? tune_trials % kPaths : path;
     }
     cudaEvent_t tune_ev[2] = {nullptr, nullptr};
+    // blocks per parent of the cloud fit, tuned on the first six steps (1, 2, 4, twice
+    // each) by the cloud-fit launches' own time, before the graph is captured
+    static constexpr int kFitSplits = 3;
+    const int fit_splits[kFitSplits] = {1, 2, 4};
+    bool fit_tuning = true;
+    int fit_trials = 0, fit_pending = -1, fit_chosen = 0;
+    double fit_ms[kFitSplits] = {0, 0, 0};
+    cudaEvent_t fit_ev[2] = {nullptr, nullptr};
     void* dev_mem = nullptr;
 
     ~Batch() override {
         if (stream) cudaStreamSynchronize(stream);
         for (cudaEvent_t e : tune_ev)
+            if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : fit_ev)
             if (e) cudaEventDestroy(e);
         if (exec) cudaGraphExecDestroy(exec);
         if (done) cudaEventDestroy(done);
@@ -1267,6 +1337,8 @@ template <typename T> struct Batch final : scphd_batch {
         CUDA_TRY(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
         CUDA_TRY(cudaEventCreate(&tune_ev[0]));
         CUDA_TRY(cudaEventCreate(&tune_ev[1]));
+        CUDA_TRY(cudaEventCreate(&fit_ev[0]));
+        CUDA_TRY(cudaEventCreate(&fit_ev[1]));
         std::vector<std::vector<int2>> mp, mpred;
         std::vector<std::vector<int4>> ml;
         stage_off.resize(F);
@@ -1383,14 +1455,21 @@ template <typename T> struct Batch final : scphd_batch {
                 LAUNCHED();
             }
         } else {
+            const bool fit_timed = fit_tuning && !capturing;
+            const int fsi = fit_timed ? fit_trials % kFitSplits : fit_chosen, split = fit_splits[fsi];
+            if (fit_timed) CUDA_TRY(cudaEventRecord(fit_ev[0], stream));
             for (const Group& g : groups) {
                 if (g.fit_p)
-                    k_cloud_fit_batch<T, KK, kFitP><<<g.n_parent, 256, fit_smem, stream>>>(*g.tab, d_fa + g.first,
-                                                                                           g.map_parent);
+                    k_cloud_fit_batch<T, KK, kFitP><<<g.n_parent * split, 256, fit_smem, stream>>>(
+                        *g.tab, d_fa + g.first, g.map_parent, split);
                 else
-                    k_cloud_fit_batch<T, KK><<<g.n_parent, 256, fit_smem, stream>>>(*g.tab, d_fa + g.first,
-                                                                                    g.map_parent);
+                    k_cloud_fit_batch<T, KK><<<g.n_parent * split, 256, fit_smem, stream>>>(*g.tab, d_fa + g.first,
+                                                                                            g.map_parent, split);
                 LAUNCHED();
+            }
+            if (fit_timed) {
+                CUDA_TRY(cudaEventRecord(fit_ev[1], stream));
+                fit_pending = fsi;
             }
             for (const Group& g : groups) {
                 k_prep_batch<T, KK><<<g.n_parent, kPrepThreads, prep_smem_bytes<T>(), stream>>>(*g.tab, d_fa + g.first,
@@ -1430,12 +1509,39 @@ template <typename T> struct Batch final : scphd_batch {
             return fail(SCPHD_ERR_CAPACITY, "the fused kernel needs more shared memory than a block has");
         if (captured) return fail(SCPHD_ERR_INVALID, "the batch's step graph is already captured");
         fused_mode = mode;
-        if (mode == 1) tuning = false;   // the stage kernels' merge shape is not needed
+        if (mode == 1) tuning = fit_tuning = false;   // the stage kernels' shapes are not needed
         return SCPHD_OK;
     }
     int fused_path() const override { return path_now() == 2 ? 1 : 0; }
+    scphd_status set_fit_split(int blocks_per_parent) override {
+        if (captured) return fail(SCPHD_ERR_INVALID, "the batch's step graph is already captured");
+        for (int k = 0; k < kFitSplits; ++k)
+            if (fit_splits[k] == blocks_per_parent) {
+                fit_tuning = false;
+                fit_pending = -1;
+                fit_chosen = k;
+                return SCPHD_OK;
+            }
+        return fail(SCPHD_ERR_INVALID, "blocks_per_parent must be 1, 2 or 4");
+    }
+    void get_fit_split(int32_t* blocks_per_parent, int32_t* tuned) const override {
+        if (blocks_per_parent) *blocks_per_parent = fit_splits[fit_chosen];
+        if (tuned) *tuned = fit_tuning ? 0 : 1;
+    }
 
     scphd_status tune_collect() {
+        if (fit_pending >= 0) {
+            CUDA_TRY(cudaEventSynchronize(fit_ev[1]));
+            float ms = 0;
+            CUDA_TRY(cudaEventElapsedTime(&ms, fit_ev[0], fit_ev[1]));
+            fit_ms[fit_pending] += ms;
+            fit_pending = -1;
+            if (++fit_trials >= 2 * kFitSplits) {
+                fit_tuning = false;
+                for (int k = 1; k < kFitSplits; ++k)
+                    if (fit_ms[k] < fit_ms[fit_chosen]) fit_chosen = k;
+            }
+        }
         if (tune_pending < 0) return SCPHD_OK;
         CUDA_TRY(cudaEventSynchronize(tune_ev[1]));
         float ms = 0;
@@ -1510,7 +1616,7 @@ template <typename T> struct Batch final : scphd_batch {
             const scphd_status ts = tune_collect();
             if (ts != SCPHD_OK) return ts;
         }
-        if (use_graph && !tuning) {
+        if (use_graph && !tuning && !fit_tuning) {
             if (!captured) {
                 cudaGraph_t g = nullptr;
                 CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
@@ -1584,6 +1690,17 @@ scphd_status scphd_batch_set_fused(scphd_batch* b, int32_t mode) {
 scphd_status scphd_batch_get_fused(scphd_batch* b, int32_t* fused) {
     if (!b || !fused) return fail(SCPHD_ERR_INVALID, "null batch or output");
     *fused = b->fused_path();
+    return SCPHD_OK;
+}
+
+scphd_status scphd_batch_set_fit_split(scphd_batch* b, int32_t blocks_per_parent) {
+    if (!b) return fail(SCPHD_ERR_INVALID, "null batch");
+    return b->set_fit_split(blocks_per_parent);
+}
+
+scphd_status scphd_batch_get_fit_split(scphd_batch* b, int32_t* blocks_per_parent, int32_t* tuned) {
+    if (!b) return fail(SCPHD_ERR_INVALID, "null batch");
+    b->get_fit_split(blocks_per_parent, tuned);
     return SCPHD_OK;
 }
 

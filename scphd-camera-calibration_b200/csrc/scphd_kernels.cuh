@@ -141,9 +141,9 @@ __global__ void k_predict_parents(__grid_constant__ const Params prm, double* ex
 }
 
 // ---------------------------------------------------------------- (b) cloud -> fit
-// One CTA per parent; each warp takes the parent's daughter Gaussians in pairs, lanes
-// 0-15 owning samples l, l+16, ... of the first and lanes 16-31 those of the second.
-// Covers: predict_features + ps (.cu:154-178, 1144-1150),
+// One CTA per parent; each warp takes every eighth of the parent's daughter Gaussians,
+// a whole warp per Gaussian, after a shared tail pass per round (the sample layout
+// below).  Covers: predict_features + ps (.cu:154-178, 1144-1150),
 // worldToDisparityKernel + computePdKernel (kernels.cu:6-47, 82-99), weight by pD
 // (.cu:1602-1609), normalizeWeightsKernel + fitGaussiansKernel (kernels.cu:996-1018,
 // 102-438) and the non-detection copy (.cu:1290-1420).
@@ -196,60 +196,74 @@ __device__ __forceinline__ void ltz_plus_mean(const double* line, const double z
     ltz_line<double, double2, 2>(line, z, y);
 }
 
-// sum over s < n (n a multiple of 4) of a[s] b[s], four partial sums, rows read in
-// 16-byte pieces (row starts are 16-byte aligned)
-__device__ __forceinline__ float moment_sweep(const float* a, const float* b, int n) {
-    const float4* a4 = reinterpret_cast<const float4*>(a);
-    const float4* b4 = reinterpret_cast<const float4*>(b);
+// sum over the samples of a[s] b[s], four partial sums over 4-sample pieces read in
+// 16 bytes (row starts are 16-byte aligned): first the nt pieces of the tail rows (ta,
+// tb), then pieces i0 .. n4-1 of the main rows (a, b) -- the order of one sweep over
+// rows holding all samples, so the sums do not depend on where samples were staged
+__device__ __forceinline__ float moment_sweep(const float* ta, const float* tb, int nt, const float* a,
+                                              const float* b, int i0, int n4) {
     float s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-    for (int i = 0; i < (n >> 2); ++i) {
-        const float4 y = a4[i], z = b4[i];
+    auto piece = [&](const float4 y, const float4 z) {
         s0 += y.x * z.x;
         s1 += y.y * z.y;
         s2 += y.z * z.z;
         s3 += y.w * z.w;
-    }
+    };
+    for (int i = 0; i < nt; ++i) piece(reinterpret_cast<const float4*>(ta)[i], reinterpret_cast<const float4*>(tb)[i]);
+    for (int i = i0; i < n4; ++i) piece(reinterpret_cast<const float4*>(a)[i], reinterpret_cast<const float4*>(b)[i]);
     return (s0 + s1) + (s2 + s3);
 }
-__device__ __forceinline__ double moment_sweep(const double* a, const double* b, int n) {
-    const double2* a2 = reinterpret_cast<const double2*>(a);
-    const double2* b2 = reinterpret_cast<const double2*>(b);
+__device__ __forceinline__ double moment_sweep(const double* ta, const double* tb, int nt, const double* a,
+                                               const double* b, int i0, int n4) {
     double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-    for (int i = 0; i < (n >> 2); ++i) {
-        const double2 y = a2[2 * i], z = b2[2 * i];
-        const double2 y1 = a2[2 * i + 1], z1 = b2[2 * i + 1];
-        s0 += y.x * z.x;
-        s1 += y.y * z.y;
+    auto piece = [&](const double* y, const double* z) {
+        const double2 y0 = reinterpret_cast<const double2*>(y)[0], z0 = reinterpret_cast<const double2*>(z)[0];
+        const double2 y1 = reinterpret_cast<const double2*>(y)[1], z1 = reinterpret_cast<const double2*>(z)[1];
+        s0 += y0.x * z0.x;
+        s1 += y0.y * z0.y;
         s2 += y1.x * z1.x;
         s3 += y1.y * z1.y;
-    }
+    };
+    for (int i = 0; i < nt; ++i) piece(ta + 4 * i, tb + 4 * i);
+    for (int i = i0; i < n4; ++i) piece(a + 4 * i, b + 4 * i);
     return (s0 + s1) + (s2 + s3);
 }
 
-// Staged sample rows: each warp works on Gaussians in pairs and stages, per Gaussian of
-// the pair, 8 rows of P4 = round_up(P, 4) values: r d for (u, v, d, vu, vv, vd), r and
-// w'.  The row stride is P4 or the next size whose rows start an odd multiple of 4
-// banks apart, so that the eight rows a lane-per-moment sweep reads at one sample
-// index (16-byte pieces) fall in distinct banks; the second Gaussian's rows start 16
-// values further on, so that the two half-warps' stores of one row never share a bank.
+// Sample layout.  A warp takes its Gaussians (j = warp, warp + 8, ...) in rounds of up
+// to 8.  With R = P mod 32 in {4, 8, 16} (P = 100: R = 4), samples [0, R) of the
+// round's 32 / R Gaussians fill one tail pass (lane = Gaussian * R + sample) and
+// samples [R, P) of each Gaussian fill whole warp passes (lane l: R + 32 t + l); with
+// any other R every sample is taken in warp passes.  So a pass has no idle lanes when
+// P = 32 m + R, and lanes of one pass share a Gaussian (no divergence) outside the
+// tail pass.  Staged rows per warp: 8 main rows of sY values (r d[6], r, w' at sample
+// index) and a tail block of 9 R values per Gaussian (the same 8 rows of R samples):
+// sY puts the eight rows a lane-per-moment sweep reads at one sample index (16-byte
+// pieces) in distinct banks, and the 9 R tail stride does the same for the tail
+// pass's stores (lanes of distinct Gaussians, same sample).
 template <typename T> __host__ __device__ constexpr int stage_stride(int P4) {
     return sizeof(T) == 4 ? ((P4 % 8 == 4) ? P4 : P4 + 4) : P4 + 2;
+}
+__host__ __device__ constexpr int fit_tail(int P) {
+    return (P % 32 == 4 || P % 32 == 8 || P % 32 == 16) ? P % 32 : 0;
 }
 // stride of a cloud's rows (x, y, z, vx, vy, vz, weight): P rounded up to 32 bytes
 template <typename T> __host__ __device__ constexpr int cloud_stride(int P) {
     return sizeof(T) == 4 ? ((P + 7) & ~7) : ((P + 3) & ~3);
 }
 constexpr int kFitWarps = 8;
-constexpr int kStageRows = 8;   // r d[6], r, w'
+constexpr int kFitRound = 8;     // Gaussians per warp and round
+constexpr int kStageRows = 8;    // r d[6], r, w'
+constexpr int kTailFloats = 288; // 32 / R Gaussians x 9 R per warp
 template <typename T> __host__ __device__ inline size_t cloud_fit_smem_bytes(int P) {
     const int P4 = (P + 3) & ~3;
-    return (size_t)kFitWarps * 2 * (kStageRows * stage_stride<T>(P4) + 16) * sizeof(T);   // sample rows
+    return (size_t)kFitWarps * (kStageRows * stage_stride<T>(P4) + kTailFloats) * sizeof(T);
 }
 
-// PC > 0: the body for exactly PC samples per feature, whose strides and loop bounds are
-// compile-time constants (immediate address offsets instead of per-sample index
-// arithmetic); PC == 0: any P.  kFitP is the specialised count (the configurations'
-// particles_per_feature); fit_specialised says whether a filter's parameters match it.
+// PC > 0: the body for exactly PC samples per feature, whose strides, loop bounds and
+// tail split are compile-time constants (immediate address offsets instead of
+// per-sample index arithmetic); PC == 0: any P.  kFitP is the specialised count (the
+// configurations' particles_per_feature); fit_specialised says whether a filter's
+// parameters match it.
 constexpr int kFitP = 100;
 template <typename T> __host__ __device__ inline bool fit_specialised(const Params& prm) {
     return prm.P == kFitP && prm.Ps == cloud_stride<T>(kFitP);
@@ -258,33 +272,42 @@ template <typename T, int K, int PC = 0>
 __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>& b, int cur, int M, int fixed,
                                                int has_pred, double dt, uint32_t pred_frame, uint32_t sample_frame,
                                                const double* zu, const double* zv, const double* zd, int p,
-                                               T* s_stage) {
-    if (p == 0 && zu != nullptr) {   // this frame's measurements into the T layout (u, v, d)
+                                               int c, int split, T* s_stage) {
+    if (p == 0 && c == 0 && zu != nullptr) {   // this frame's measurements into the T layout (u, v, d)
         for (int mm = threadIdx.x; mm < M; mm += blockDim.x) {
             b.z[mm * 3 + 0] = (T)zu[mm];
             b.z[mm * 3 + 1] = (T)zv[mm];
             b.z[mm * 3 + 2] = (K == 3 && zd) ? (T)zd[mm] : T(0);
         }
     }
+    // the parent's Gaussians are shared by the warps of its `split` blocks: block c's
+    // warp w takes j = gw, gw + nwp, ... (gw = c * kFitWarps + w, nwp = split * kFitWarps)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int gw = c * kFitWarps + warp, nwp = split * kFitWarps;
     const int row = b.src[p];
     const int G = min(b.map_n[cur][row], prm.Gcap);
     const int P = PC > 0 ? PC : prm.P, Ps = PC > 0 ? cloud_stride<T>(PC) : prm.Ps;
     const int P4 = (P + 3) & ~3;
     const int sY = stage_stride<T>(P4);
-    T* Ywarp = s_stage + (size_t)warp * 2 * (kStageRows * sY + 16);   // per Gaussian of the pair: r d[6], r, w'
-    __shared__ T s_shift[kFitWarps * 2 * 6];   // per warp and Gaussian: the moments' shift
+    const int R = fit_tail(P);                      // tail samples per Gaussian (0: no tail pass)
+    const int TG = R ? 32 / R : kFitRound;          // Gaussians per round
+    T* Y = s_stage + (size_t)warp * kStageRows * sY;                                   // main rows
+    T* Yt = s_stage + (size_t)kFitWarps * kStageRows * sY + (size_t)warp * kTailFloats;  // tail blocks
+    __shared__ T s_shift[kFitWarps * kFitRound * 6];          // per warp and Gaussian of the round
+    __shared__ __align__(16) T s_L[kFitWarps * kFitRound * 28];  // Cholesky factor and mean of merged ones
     __shared__ Pose<T> pose_upd, pose_src;
     __shared__ int s_rd, s_wr;
-    __shared__ __align__(16) T s_L[kFitWarps * 2 * 28];   // per warp and Gaussian: Cholesky factor and mean
     __shared__ T s_fit[kFitWarps * 32];  // per warp: the fitted row (W, pD, mean[6], cov[21])
     if (threadIdx.x == 0) {
         double zero[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         pose_upd = make_pose<T>(fixed ? zero : b.ext + 12 * p);
         pose_src = make_pose<T>(b.map_ext[cur] + 12 * row);
-        b.surv_n[p] = 0;
-        atomicAdd(&b.counters[4], (unsigned long long)G * (unsigned long long)M);
-        atomicAdd(&b.counters[6], (unsigned long long)G * (unsigned long long)M);
+        if (c == 0) {
+            b.surv_n[p] = 0;
+            atomicAdd(&b.counters[4], (unsigned long long)G * (unsigned long long)M);
+            atomicAdd(&b.counters[6], (unsigned long long)G * (unsigned long long)M);
+            atomicAdd(&b.counters[10], (unsigned long long)G);
+        }
         s_rd = 0;
         s_wr = 0;
     }
@@ -292,7 +315,10 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
     const Model& m = prm.model;
     const T invP = T(1) / T(P);
     const T dtT = (T)dt, half_dt2 = T(0.5) * (T)dt * (T)dt;
+    const T min_w = (T)prm.min_weight;
     T* fitw = s_fit + warp * 32;
+    T* shw = s_shift + warp * kFitRound * 6;
+    T* Lw = s_L + warp * kFitRound * 28;
     // moment owned by this lane: rows (ra, rb) of the product Y[ra] * Y[rb]: lane 0
     // S0 = sum r r, lane 1 S2 = sum w' w', lanes 2-7 S1 = sum r (r d), lanes 8-28 SS
     int ra = 6, rb = 6;
@@ -304,148 +330,198 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
         ra = aa;
         rb = e - aa * (aa + 1) / 2;
     }
-    for (int j0 = 2 * warp; j0 < G; j0 += 2 * kFitWarps) {
-        const int nG = min(2, G - j0);
-        // the pair's entries (map order keeps merged components first, so a pair is
-        // nearly always of one kind and the sample loop does not diverge)
-        int refg[2] = {0, 0};
-        T Wg[2] = {T(0), T(0)};
+    // one sample s of Gaussian j (entry ref, factor line Lg): the predicted particle X,
+    // its measurement y; returns the sample weight omega (1/P for a drawn sample)
+    auto sample = [&](int ref, int j, int s, const T* Lg, T (&X)[6], T (&y)[6]) -> T {
+        T om;
+        if (ref < 0) {   // merged component: draw (.cu:640-690) and map to world (.cu:1222-1286)
+            const uint32_t key_i = (uint32_t)(-1 - ref);
+            uint32_t w0[4], w1[4];
+            philox_rk((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 0), prm.rk, w0);
+            philox_rk((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 1), prm.rk, w1);
+            T z[6];
+            Pair<T>::two(w0[0], w0[1], z[0], z[1]);
+            Pair<T>::two(w0[2], w0[3], z[2], z[3]);
+            Pair<T>::two(w1[0], w1[1], z[4], z[5]);
+            T yy[6];
+            ltz_plus_mean(Lg, z, yy);   // y = L z + mean
+            invert(yy, pose_src, m, X);
+            om = invP;
+        } else {         // non-detection cloud carried from the previous frame
+            // the previous frame's clouds are only read in this kernel (writes go to
+            // the other buffer): read-only loads, free to move ahead of the stores
+            const T* cl_in = b.cloud[cur] + (size_t)ref * 7 * Ps;
 #pragma unroll
-        for (int g = 0; g < 2; ++g) {   // static indices: refg and Wg stay in registers
-            if (g >= nG) break;
-            const size_t erow = (size_t)row * prm.Gcap + j0 + g;
-            const T* ent = b.map[cur] + erow * kRow;
-            const int ref = b.map_ref[cur][erow];
-            refg[g] = ref;
-            Wg[g] = has_pred ? ent[0] * (T)prm.ps : ent[0];
-            T* Lw = s_L + (warp * 2 + g) * 28;
-            if (ref < 0) {   // Cholesky factor (21, stored in the map row) and mean (6) of the merged component
-                if (lane < 21) Lw[lane] = ent[7 + lane];
-                else if (lane < 27) Lw[lane] = ent[1 + lane - 21];
-                else if (lane == 27) Lw[27] = T(0);
-            } else if (lane == 0) {
-                atomicAdd(&s_rd, 1);
+            for (int a2 = 0; a2 < 6; ++a2) X[a2] = __ldg(cl_in + a2 * Ps + s);
+            om = __ldg(cl_in + 6 * Ps + s);
+        }
+        if (has_pred) {   // predict_features with feature noise
+            uint32_t w[4];
+            philox_rk((uint32_t)s, (uint32_t)j, (uint32_t)p, ctr_word3(pred_frame, ST_FEAT, 0), prm.rk, w);
+            T z[4];
+            Pair<T>::two(w[0], w[1], z[0], z[1]);
+            Pair<T>::two(w[2], w[3], z[2], z[3]);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                T a2 = (T)prm.feat_std[q] * z[q];
+                X[q] = X[q] + X[q + 3] * dtT + a2 * half_dt2;
+                X[q + 3] = X[q + 3] + a2 * dtT;
             }
         }
+        measure(X, pose_upd, m, y);
+        return om;
+    };
+    // the non-detection cloud candidate: predicted world point, weight 1 - pD
+    auto write_nd = [&](int j, int s, const T (&X)[6], T pds) {
+        T* cl_out = b.cloud[cur ^ 1] + ((size_t)p * prm.Gcap + j) * 7 * Ps;
+#pragma unroll
+        for (int a2 = 0; a2 < 6; ++a2) __stcs(cl_out + a2 * Ps + s, X[a2]);
+        __stcs(cl_out + 6 * Ps + s, T(1) - pds);
+    };
+    // staged moment rows of one sample (zero-weight samples and the padding stage zeros)
+    auto stage = [&](T* Ys, int stride, const T (&y)[6], const T (&shift)[6], T wp) {
+        const T r = wp != T(0) ? weight_root(wp) : T(0);
+#pragma unroll
+        for (int a2 = 0; a2 < 6; ++a2) Ys[a2 * stride] = wp != T(0) ? r * (y[a2] - shift[a2]) : T(0);
+        Ys[6 * stride] = r;
+        Ys[7 * stride] = wp;
+    };
+    const int nW = G > gw ? (G - gw + nwp - 1) / nwp : 0;   // this warp's Gaussians
+    for (int k0 = 0; k0 < nW; k0 += TG) {
+        const int nR = min(TG, nW - k0);
+        // lane k < nR: entry of the round's Gaussian k
+        int my_ref = 0;
+        T my_W = T(0);
+        if (lane < nR) {
+            const size_t erow = (size_t)row * prm.Gcap + gw + nwp * (k0 + lane);
+            my_ref = b.map_ref[cur][erow];
+            my_W = has_pred ? b.map[cur][erow * kRow] * (T)prm.ps : b.map[cur][erow * kRow];
+        }
+        const unsigned merged = __ballot_sync(0xffffffffu, lane < nR && my_ref < 0);
+        const unsigned writes = __ballot_sync(0xffffffffu, lane < nR && my_W >= min_w);
+        if (lane == 0) {
+            atomicAdd(&s_rd, nR - __popc(merged));
+            atomicAdd(&s_wr, __popc(writes));
+        }
+        for (unsigned mk = merged; mk; mk &= mk - 1) {   // Cholesky factor (21, stored in the map row) and mean (6)
+            const int k = __ffs(mk) - 1;
+            const T* ent = b.map[cur] + ((size_t)row * prm.Gcap + gw + nwp * (k0 + k)) * kRow;
+            T* Lk = Lw + k * 28;
+            if (lane < 21) Lk[lane] = ent[7 + lane];
+            else if (lane < 27) Lk[lane] = ent[1 + lane - 21];
+            else if (lane == 27) Lk[27] = T(0);
+        }
         __syncwarp();
-        // lanes 0-15 sample Gaussian j0, lanes 16-31 Gaussian j0 + 1, 16 samples each per pass
-        const int g = lane >> 4, hl = lane & 15;
-        const bool gvalid = g < nG;
-        const int ref = g ? refg[1] : refg[0];
-        const int j = j0 + g;
-        const bool wnd = (g ? Wg[1] : Wg[0]) >= (T)prm.min_weight;
-        T* Y = Ywarp + (size_t)g * (kStageRows * sY + 16);
-        T* shift_g = s_shift + (warp * 2 + g) * 6;
-        int n_in = 0;
-        bool any = false;
-        // raw = false: stage the moment rows (see above) and write the non-detection
-        // clouds; raw = true (fallback fit only): stage y itself where `stage`, write nothing
-        auto sample_pass = [&](bool raw, bool stage) {
-            n_in = 0;
-            any = false;
+        // tail pass: samples [0, R) of the round's Gaussians; lane gi * R (sample 0)
+        // gives its Gaussian's shift
+        int t_in = 0;
+        bool t_any = false;
+        if (R) {
+            const int gi = lane / R, s = lane - gi * R;
+            const bool valid = gi < nR;
+            const int ref = __shfl_sync(0xffffffffu, my_ref, gi & 31);
+            const bool wnd = __shfl_sync(0xffffffffu, my_W, gi & 31) >= min_w;
+            const int j = gw + nwp * (k0 + gi);
+            T X[6], y[6], om = 0;
+            if (valid) {
+                om = sample(ref, j, s, Lw + gi * 28, X, y);
+            } else {
+#pragma unroll
+                for (int a2 = 0; a2 < 6; ++a2) { X[a2] = 0; y[a2] = 0; }
+            }
+            const bool inr = valid && in_range(y, m);
+            const T pds = inr ? (T)m.pd : T(0);
+            if (valid && wnd) write_nd(j, s, X, pds);
+            const T wp = om * pds;
             T shift[6];
-            for (int t = 0; 16 * t < P4; ++t) {
-                const int s = 16 * t + hl;
-                const bool valid = gvalid && s < P;
-                T X[6], om = 0, y[6];
+#pragma unroll
+            for (int a2 = 0; a2 < 6; ++a2) {
+                const T v = __shfl_sync(0xffffffffu, y[a2], lane - s);
+                shift[a2] = isfinite(v) ? v : T(0);
+            }
+            if (valid && s == 0) {
+#pragma unroll
+                for (int a2 = 0; a2 < 6; ++a2) shw[gi * 6 + a2] = shift[a2];
+            }
+            stage(Yt + gi * 9 * R + s, R, y, shift, wp);
+            const unsigned gm = (R == 32 ? 0xffffffffu : ((1u << R) - 1u)) << (gi * R & 31);
+            t_in = __popc(__ballot_sync(0xffffffffu, inr) & gm);
+            t_any = (__ballot_sync(0xffffffffu, wp != T(0)) & gm) != 0u;
+        }
+        __syncwarp();
+        for (int k = 0; k < nR; ++k) {
+            const int j = gw + nwp * (k0 + k);
+            const int ref = __shfl_sync(0xffffffffu, my_ref, k);
+            const T W = __shfl_sync(0xffffffffu, my_W, k);
+            const bool wnd = W >= min_w;
+            const T* Lg = Lw + k * 28;
+            const T* Ytk = Yt + k * 9 * R;
+            T shift[6];
+            if (R) {
+#pragma unroll
+                for (int a2 = 0; a2 < 6; ++a2) shift[a2] = shw[k * 6 + a2];
+            }
+            int n_in = R ? __shfl_sync(0xffffffffu, t_in, (k * R) & 31) : 0;
+            bool any = R ? __shfl_sync(0xffffffffu, (int)t_any, (k * R) & 31) != 0 : false;
+            // warp passes over samples [R, P4): moment rows, non-detection clouds
+            for (int s0 = R; s0 < P4; s0 += 32) {
+                const int s = s0 + lane;
+                const bool valid = s < P;
+                T X[6], y[6], om = 0;
                 if (valid) {
-                    if (ref < 0) {   // merged component: draw (.cu:640-690) and map to world (.cu:1222-1286)
-                        const uint32_t key_i = (uint32_t)(-1 - ref);
-                        uint32_t w0[4], w1[4];
-                        philox_rk((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 0), prm.rk, w0);
-                        philox_rk((uint32_t)s, key_i, (uint32_t)row, ctr_word3(sample_frame, ST_SAMPLE, 1), prm.rk, w1);
-                        T z[6];
-                        Pair<T>::two(w0[0], w0[1], z[0], z[1]);
-                        Pair<T>::two(w0[2], w0[3], z[2], z[3]);
-                        Pair<T>::two(w1[0], w1[1], z[4], z[5]);
-                        T yy[6];
-                        ltz_plus_mean(s_L + (warp * 2 + g) * 28, z, yy);   // y = L z + mean
-                        invert(yy, pose_src, m, X);
-                        om = invP;
-                    } else {         // non-detection cloud carried from the previous frame
-                        // the previous frame's clouds are only read in this kernel (writes go to
-                        // the other buffer): read-only loads, free to move ahead of the stores
-                        const T* cl_in = b.cloud[cur] + (size_t)ref * 7 * Ps;
-#pragma unroll
-                        for (int a2 = 0; a2 < 6; ++a2) X[a2] = __ldg(cl_in + a2 * Ps + s);
-                        om = __ldg(cl_in + 6 * Ps + s);
-                    }
-                    if (has_pred) {   // predict_features with feature noise
-                        uint32_t w[4];
-                        philox_rk((uint32_t)s, (uint32_t)j, (uint32_t)p, ctr_word3(pred_frame, ST_FEAT, 0), prm.rk, w);
-                        T z[4];
-                        Pair<T>::two(w[0], w[1], z[0], z[1]);
-                        Pair<T>::two(w[2], w[3], z[2], z[3]);
-#pragma unroll
-                        for (int q = 0; q < 3; ++q) {
-                            T a2 = (T)prm.feat_std[q] * z[q];
-                            X[q] = X[q] + X[q + 3] * dtT + a2 * half_dt2;
-                            X[q + 3] = X[q + 3] + a2 * dtT;
-                        }
-                    }
-                    measure(X, pose_upd, m, y);
+                    om = sample(ref, j, s, Lg, X, y);
                 } else {
 #pragma unroll
                     for (int a2 = 0; a2 < 6; ++a2) { X[a2] = 0; y[a2] = 0; }
                 }
                 const bool inr = valid && in_range(y, m);
                 const T pds = inr ? (T)m.pd : T(0);
-                n_in += __popc(__ballot_sync(0xffffffffu, inr) & (g ? 0xffff0000u : 0x0000ffffu));
-                if (!raw && valid && wnd) {   // non-detection cloud candidate: predicted world point, weight 1 - pD
-                    T* cl_out = b.cloud[cur ^ 1] + ((size_t)p * prm.Gcap + j) * 7 * Ps;
-#pragma unroll
-                    for (int a2 = 0; a2 < 6; ++a2) __stcs(cl_out + a2 * Ps + s, X[a2]);
-                    __stcs(cl_out + 6 * Ps + s, T(1) - pds);
-                }
+                n_in += __popc(__ballot_sync(0xffffffffu, inr));
+                if (valid && wnd) write_nd(j, s, X, pds);
                 const T wp = om * pds;
-                any |= wp != T(0);
-                if (t == 0) {   // shift: the Gaussian's first sample (lane 0 or 16), if finite, else 0
+                any |= __any_sync(0xffffffffu, wp != T(0));
+                if (!R && s0 == 0) {   // shift: the Gaussian's first sample, if finite, else 0
 #pragma unroll
                     for (int a2 = 0; a2 < 6; ++a2) {
-                        const T v = __shfl_sync(0xffffffffu, y[a2], lane & 16);
+                        const T v = __shfl_sync(0xffffffffu, y[a2], 0);
                         shift[a2] = isfinite(v) ? v : T(0);
                     }
-                    if (gvalid) {   // static indices: the shift stays in registers
+                    if (lane < 6) {   // static indices: the shift stays in registers
 #pragma unroll
                         for (int a2 = 0; a2 < 6; ++a2)
-                            if (hl == a2) shift_g[a2] = shift[a2];
+                            if (lane == a2) shw[k * 6 + a2] = shift[a2];
                     }
                 }
-                if (stage && gvalid && s < P4) {
-                    if (raw) {
+                if (s < P4) stage(Y + s, sY, y, shift, wp);
+            }
+            const T pbar = (T)((double)n_in * m.pd / (double)P);
+            const bool raw = !any && n_in > 0 && m.pd > 0.0;
+            if (raw) {
+                // the fallback fit (below) needs the raw samples: rare, so they are drawn
+                // again, every sample in warp passes, y itself staged in the main rows
+                __syncwarp();
+                for (int s0 = 0; s0 < P4; s0 += 32) {
+                    const int s = s0 + lane;
+                    T X[6], y[6];
+                    if (s < P) {
+                        sample(ref, j, s, Lg, X, y);
+                    } else {
+#pragma unroll
+                        for (int a2 = 0; a2 < 6; ++a2) y[a2] = 0;
+                    }
+                    if (s < P4) {
 #pragma unroll
                         for (int a2 = 0; a2 < 6; ++a2) Y[a2 * sY + s] = y[a2];
-                    } else {   // r d and r = sqrt(w'); zero-weight samples (and the padding) stage zeros
-                        const T r = wp != T(0) ? weight_root(wp) : T(0);
-#pragma unroll
-                        for (int a2 = 0; a2 < 6; ++a2) Y[a2 * sY + s] = wp != T(0) ? r * (y[a2] - shift[a2]) : T(0);
-                        Y[6 * sY + s] = r;
-                        Y[7 * sY + s] = wp;
                     }
                 }
             }
-        };
-        sample_pass(false, true);
-        if (lane == 0) atomicAdd(&s_wr, (int)(Wg[0] >= (T)prm.min_weight) + (nG > 1 ? (int)(Wg[1] >= (T)prm.min_weight) : 0));
-        const bool any0 = __any_sync(0xffffffffu, any && g == 0), any1 = __any_sync(0xffffffffu, any && g == 1);
-        const int n_in0 = __shfl_sync(0xffffffffu, n_in, 0), n_in1 = __shfl_sync(0xffffffffu, n_in, 16);
-        // the fallback fit (below) needs the raw samples: rare, so they are drawn again
-        const bool raw0 = !any0 && n_in0 > 0 && m.pd > 0.0, raw1 = nG > 1 && !any1 && n_in1 > 0 && m.pd > 0.0;
-        if (raw0 || raw1) {
             __syncwarp();
-            sample_pass(true, g ? raw1 : raw0);
-        }
-        __syncwarp();
-        for (int gg = 0; gg < nG; ++gg) {
-            const int jj = j0 + gg;
-            const T W = gg ? Wg[1] : Wg[0];
-            const T* Yg = Ywarp + (size_t)gg * (kStageRows * sY + 16);
-            const T* sh = s_shift + (warp * 2 + gg) * 6;
-            const bool any_w = gg ? any1 : any0;
-            const T pbar = (T)((double)(gg ? n_in1 : n_in0) * m.pd / (double)P);
-            if (any_w) {
+            const T* sh = shw + k * 6;
+            if (any) {
                 // lane q < 29: moment q over the samples, four partial sums
-                const T mom = lane < 29 ? moment_sweep(Yg + ra * sY, Yg + rb * sY, P4) : T(0);
+                const T mom = lane < 29 ? moment_sweep(Ytk + ra * R, Ytk + rb * R, R / 4, Y + ra * sY, Y + rb * sY,
+                                                       R / 4, P4 / 4)
+                                        : T(0);
                 const T S0 = __shfl_sync(0xffffffffu, mom, 0), S2 = __shfl_sync(0xffffffffu, mom, 1);
                 const T inv = T(1) / S0, scale = T(1) + S2 * inv * inv;
                 // lanes 2-7 hold S1 (the mean offsets), lanes 8-28 hold SS
@@ -466,7 +542,7 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
                 // samples) and covariance x (P + P)/P over the valid samples (raw rows)
                 T mu = 0;
                 if (lane < 6) {
-                    for (int s = 0; s < P; ++s) mu += Yg[lane * sY + s];
+                    for (int s = 0; s < P; ++s) mu += Y[lane * sY + s];
                 }
                 T mus[6];
 #pragma unroll
@@ -479,7 +555,7 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
                         if (ra == a2) ma = mus[a2];
                         if (rb == a2) mb = mus[a2];
                     }
-                    for (int s = 0; s < P; ++s) cva += (Yg[ra * sY + s] - ma) * (Yg[rb * sY + s] - mb);
+                    for (int s = 0; s < P; ++s) cva += (Y[ra * sY + s] - ma) * (Y[rb * sY + s] - mb);
                 }
                 const T scale = (T(P) * T(P) + T(P)) / T(P);
                 if (lane < 6) fitw[2 + lane] = mu;
@@ -493,7 +569,7 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
             if (lane == 1) fitw[1] = pbar;
             __syncwarp();
             // fitted row: lane q writes element q (W, pD, mean[6], packed cov[21])
-            T* fr = b.fit + ((size_t)p * prm.Gcap + jj) * kRow;
+            T* fr = b.fit + ((size_t)p * prm.Gcap + j) * kRow;
             if (lane < 29) fr[lane] = fitw[lane];
             __syncwarp();
         }
@@ -502,29 +578,32 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
     if (threadIdx.x == 0) {
         atomicAdd(&b.counters[8], (unsigned long long)s_rd);
         atomicAdd(&b.counters[9], (unsigned long long)s_wr);
-        atomicAdd(&b.counters[10], (unsigned long long)G);
     }
 }
 
 
+// grid: `split` blocks per parent (block x: parent x / split, part x % split)
 template <typename T, int K, int PC = 0>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
     k_cloud_fit(__grid_constant__ const Params prm, __grid_constant__ const Bufs<T> b, int cur, int M, int fixed,
                 int has_pred, double dt, uint32_t pred_frame, uint32_t sample_frame, const double* zu,
-                const double* zv, const double* zd) {
+                const double* zv, const double* zd, int split) {
     extern __shared__ __align__(16) unsigned char dsm_fit[];
-    cloud_fit_body<T, K, PC>(prm, b, cur, M, fixed, has_pred, dt, pred_frame, sample_frame, zu, zv, zd, blockIdx.x,
-                         reinterpret_cast<T*>(dsm_fit));
+    const int p = blockIdx.x / split;
+    cloud_fit_body<T, K, PC>(prm, b, cur, M, fixed, has_pred, dt, pred_frame, sample_frame, zu, zv, zd, p,
+                             blockIdx.x - p * split, split, reinterpret_cast<T*>(dsm_fit));
 }
 
 template <typename T, int K, int PC = 0>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
-    k_cloud_fit_batch(const __grid_constant__ SlotTable<T> tab, const FrameArgs* fas, const int2* map) {
+    k_cloud_fit_batch(const __grid_constant__ SlotTable<T> tab, const FrameArgs* fas, const int2* map, int split) {
     extern __shared__ __align__(16) unsigned char dsm_fit[];
-    const int2 fp = map[blockIdx.x];
+    const int q = blockIdx.x / split;
+    const int2 fp = map[q];
     const FrameArgs fa = fas[fp.x];
     cloud_fit_body<T, K, PC>(tab.prm[fp.x], tab.b[fp.x], fa.cur, fa.M, fa.fixed, fa.has_pred, fa.dt, fa.pred_frame,
-                         fa.sample_frame, fa.zu, fa.zv, fa.zd, fp.y, reinterpret_cast<T*>(dsm_fit));
+                             fa.sample_frame, fa.zu, fa.zv, fa.zd, fp.y, blockIdx.x - q * split, split,
+                             reinterpret_cast<T*>(dsm_fit));
 }
 
 // ---------------------------------------------------------------- (c0) Kalman terms
@@ -1813,7 +1892,7 @@ template <typename T, int K>
 __device__ __forceinline__ void fused_parent(const Params& prm, const Bufs<T>& b, const FrameArgs& fa, int p,
                                              unsigned char* smem) {
     cloud_fit_body<T, K>(prm, b, fa.cur, fa.M, fa.fixed, fa.has_pred, fa.dt, fa.pred_frame, fa.sample_frame, nullptr,
-                         nullptr, nullptr, p, reinterpret_cast<T*>(smem));
+                         nullptr, nullptr, p, 0, 1, reinterpret_cast<T*>(smem));
     __syncthreads();
     prep_body<T, K>(prm, b, fa.cur, p, reinterpret_cast<T*>(smem));
     for (int mb = 0; mb * (int)blockDim.x < fa.M; ++mb) {

@@ -208,6 +208,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "scphd_get_fused": (i32, [vp, P(i32)]),
         "scphd_batch_set_fused": (i32, [vp, i32]),
         "scphd_batch_get_fused": (i32, [vp, P(i32)]),
+        "scphd_set_fit_split": (i32, [vp, i32]),
+        "scphd_get_fit_split": (i32, [vp, P(i32), P(i32)]),
+        "scphd_batch_set_fit_split": (i32, [vp, i32]),
+        "scphd_batch_get_fit_split": (i32, [vp, P(i32), P(i32)]),
         "scphd_config_from_file": (i32, [ctypes.c_char_p, P(ScphdConfig), P(ScphdRunOptions)]),
         "scphd_read_mat_frames": (i32, [ctypes.c_char_p, ctypes.c_char_p, P(i32), P(i32), P(i32), P(d), i64]),
         "scphd_write_mat": (i32, [vp, ctypes.c_char_p, i32]),
@@ -391,8 +395,14 @@ class SCPHDCameraCalibration:
         _check(self._lib.scphd_get_launch_shapes(self._h, ctypes.byref(mt), ctypes.byref(lf), ctypes.byref(tuned)))
         fz = ctypes.c_int32(0)
         _check(self._lib.scphd_get_fused(self._h, ctypes.byref(fz)))
+        sp, st = ctypes.c_int32(0), ctypes.c_int32(0)
+        _check(self._lib.scphd_get_fit_split(self._h, ctypes.byref(sp), ctypes.byref(st)))
         return {"merge_threads": mt.value, "likelihood_full": bool(lf.value), "tuned": bool(tuned.value),
-                "fused": bool(fz.value)}
+                "fused": bool(fz.value), "fit_blocks_per_parent": sp.value, "fit_tuned": bool(st.value)}
+
+    def set_fit_split(self, blocks_per_parent: int) -> None:
+        """Cloud-fit blocks per parent (1, 2 or 4); fixes it instead of tuning it."""
+        _check(self._lib.scphd_set_fit_split(self._h, int(blocks_per_parent)))
 
     def set_fused(self, mode: int) -> None:
         """Update path: 0 one kernel per stage (default), 1 the fused kernel."""
@@ -565,6 +575,15 @@ class SCPHDBatch:
         fz = ctypes.c_int32(0)
         _check(self._lib.scphd_batch_get_fused(self._h, ctypes.byref(fz)))
         return bool(fz.value)
+
+    def set_fit_split(self, blocks_per_parent: int) -> None:
+        """Cloud-fit blocks per parent (1, 2 or 4) before the first graph capture."""
+        _check(self._lib.scphd_batch_set_fit_split(self._h, int(blocks_per_parent)))
+
+    def fit_split(self) -> dict:
+        sp, st = ctypes.c_int32(0), ctypes.c_int32(0)
+        _check(self._lib.scphd_batch_get_fit_split(self._h, ctypes.byref(sp), ctypes.byref(st)))
+        return {"fit_blocks_per_parent": sp.value, "fit_tuned": bool(st.value)}
 
     def synchronize(self) -> None:
         for f in self.filters:

@@ -18,7 +18,8 @@ def test_tuned_shapes_leave_results_unchanged(pkg, precision):
                                   precision=precision, calib=sc.calib, seed=61, particles_per_feature=40)
     tuned, plain = pkg.SCPHDCameraCalibration(cfg), pkg.SCPHDCameraCalibration(cfg)
     plain.set_autotune(False)
-    assert plain.launch_shapes() == {"merge_threads": 256, "likelihood_full": True, "tuned": True, "fused": False}
+    assert plain.launch_shapes() == {"merge_threads": 256, "likelihood_full": True, "tuned": True, "fused": False,
+                                     "fit_blocks_per_parent": 1, "fit_tuned": True}
     assert not tuned.launch_shapes()["tuned"]
     for k, z in enumerate(sc.frames):
         for f in (tuned, plain):
@@ -31,6 +32,44 @@ def test_tuned_shapes_leave_results_unchanged(pkg, precision):
             assert np.array_equal(tuned.mixture(1, p), plain.mixture(1, p)), f"frame {k} parent {p}"
     s = tuned.launch_shapes()
     assert s["tuned"] and s["merge_threads"] in (128, 256)
+    assert s["fit_tuned"] and s["fit_blocks_per_parent"] in (1, 2, 4)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_fit_split_leaves_results_unchanged(pkg, precision):
+    """The cloud fit with 1, 2 and 4 blocks per parent (the parent's Gaussians dealt out
+    over 8, 16 or 32 warps) gives identical states, maps and mixtures: at 100 samples per
+    feature (the specialised kernel, tail pass of 4 samples x 8 Gaussians), 72 (tail of
+    8 samples x 4 Gaussians) and 50 (no tail pass)."""
+    if not gpu_available():
+        pytest.skip("no CUDA device")
+    for P in (100, 72, 50):
+        sc = pkg.scene.make_scene(n_landmarks=40, n_frames=6, clutter_rate=10.0, seed=pkg.scene.scene_seed(6, P))
+        cfg = pkg.scene.filter_config(n_parents=48, max_gaussians=96, max_meas=128, clutter_rate=10.0,
+                                      precision=precision, calib=sc.calib, seed=P, particles_per_feature=P)
+        fs = [pkg.SCPHDCameraCalibration(cfg) for _ in range(3)]
+        for f, split in zip(fs, (1, 2, 4)):
+            f.set_fit_split(split)
+            assert f.launch_shapes()["fit_blocks_per_parent"] == split
+        for k, z in enumerate(sc.frames):
+            for f in fs:
+                f.predict(pkg.scene.DT)
+                f.update(z[:, 0], z[:, 1], fixed_camera=sc.fixed[k], d=z[:, 2])
+            ref = fs[0]
+            st0, lw0 = ref.particles()
+            for f in fs[1:]:
+                st, lw = f.particles()
+                assert np.array_equal(st, st0) and np.array_equal(lw, lw0), f"P {P} frame {k}"
+                assert np.array_equal(f.map_sizes(), ref.map_sizes()), f"P {P} frame {k} map sizes"
+                assert np.array_equal(f.counters(), ref.counters()), f"P {P} frame {k} counters"
+                for p in range(cfg.n_parents):
+                    assert np.array_equal(f.mixture(0, p), ref.mixture(0, p)), f"P {P} frame {k} parent {p} fitted"
+                    assert np.array_equal(f.mixture(1, p), ref.mixture(1, p)), f"P {P} frame {k} parent {p} merged"
+                    assert np.array_equal(f.map_weights(p), ref.map_weights(p)), f"P {P} frame {k} parent {p} map"
+            for f in fs:
+                f.resample()
+        for f in fs:
+            f.close()
 
 
 @pytest.mark.parametrize("precision", [0, 1])

@@ -117,10 +117,12 @@ def test_fp64_frames_match_oracle(pkg, orc, meas_dim):
     assert c[0] == 0 and c[1] == 0, f"capacity hit in a parity scene: {c}"
 
 
-@pytest.mark.parametrize("particles", [7, 33])
+@pytest.mark.parametrize("particles", [7, 33, 36, 72])
 def test_fp64_frames_match_oracle_sample_counts(pkg, orc, particles):
-    """Sample counts that leave a 16-sample pass of a half-warp partly filled (P = 7)
-    or reach one sample into a third pass (P = 33), both padded to 4-sample rows."""
+    """Sample counts that leave a warp pass partly filled (P = 7, padded to a 4-sample
+    row) or reach one sample into a second pass (P = 33), and counts of 32 m + 4 and
+    32 m + 8 (P = 36, 72), whose first 4 or 8 samples of 8 or 4 Gaussians share a tail
+    pass (P = 48 elsewhere: a tail of 16; P = 100, the specialised kernel: 4)."""
     _need_gpu()
     sc = pkg.scene.make_scene(n_landmarks=16, n_frames=6, clutter_rate=4.0, seed=pkg.scene.scene_seed(0, 12))
     cfg = pkg.scene.filter_config(n_parents=24, max_gaussians=160, max_meas=96, clutter_rate=4.0,
@@ -137,12 +139,13 @@ def test_fp64_frames_match_oracle_sample_counts(pkg, orc, particles):
 
 
 def test_fp64_largest_sample_count_matches_oracle(pkg, orc):
-    """216 samples per Gaussian, the most whose FP64 sample rows fit one cloud-fit
-    block's shared memory; 217 is refused at create, as is more than 256 in FP32."""
+    """256 samples per Gaussian, the largest particles_per_feature, in FP64 (whose
+    sample rows take the most shared memory per cloud-fit block; 256 = 8 x 32, so every
+    sample is taken in warp passes); more than 256 is refused at create, in FP32 too."""
     _need_gpu()
     sc = pkg.scene.make_scene(n_landmarks=12, n_frames=4, clutter_rate=3.0, seed=pkg.scene.scene_seed(0, 14))
     cfg = pkg.scene.filter_config(n_parents=8, max_gaussians=64, max_meas=64, clutter_rate=3.0,
-                                  precision=pkg.SCPHD_FP64, calib=sc.calib, seed=14, particles_per_feature=216)
+                                  precision=pkg.SCPHD_FP64, calib=sc.calib, seed=14, particles_per_feature=256)
     gpu, ref = _pair(pkg, orc, cfg)
     for k in range(sc.n_frames):
         z = sc.frames[k]
@@ -152,10 +155,9 @@ def test_fp64_largest_sample_count_matches_oracle(pkg, orc):
         _compare_frame(gpu, ref, z.shape[0], k)
         assert gpu.resample() == ref.resample(), f"frame {k} resample decision"
     big = cfg.copy()
-    big.particles_per_feature = 217
-    with pytest.raises(pkg.ScphdError) as e:
+    big.particles_per_feature = 257
+    with pytest.raises(pkg.ScphdError):
         pkg.SCPHDCameraCalibration(big)
-    assert e.value.status == 3
     fp32 = cfg.copy()
     fp32.precision = pkg.SCPHD_FP32
     fp32.particles_per_feature = 256
