@@ -202,8 +202,9 @@ scphd_status scphd_get_fused(scphd_filter* f, int32_t* fused);
  * parent's daughter Gaussians are dealt out over the warps of all its blocks (a warp
  * per Gaussian), so 2 or 4 blocks per parent fill the GPU when a filter has few
  * parents (256 blocks leave most of 148 SMs x 4 block slots idle).  By default the
- * first updates with measurements time the cloud-fit launch at each split (twice) and
- * keep the fastest; scphd_set_fit_split fixes one (and ends that tuning),
+ * updates with measurements after the first 16 (when the maps have grown) time the
+ * cloud-fit launch at each split (twice) and keep the fastest; until then the split is
+ * 1.  scphd_set_fit_split fixes one (and ends that tuning),
  * scphd_set_autotune(f, 0) fixes 1.  Results do not depend on the split.  *tuned = 1
  * once a choice is made.  No reference counterpart (fitGaussiansKernel runs a block
  * per Gaussian, src/kernels.cu:102-438). */

@@ -112,12 +112,14 @@ struct scphd_filter {
     int chosen = 0;
     cudaEvent_t tune_ev[2] = {nullptr, nullptr};
     // Blocks per parent of the cloud fit (the parent's Gaussians dealt out over the warps
-    // of all its blocks): 1, 2 or 4, tuned on the same first updates by the cloud-fit
-    // launch's own event time (each twice), or fixed by scphd_set_fit_split.  Every
-    // split computes the same values.
-    static constexpr int kFitSplits = 3;
+    // of all its blocks): 1, 2 or 4, tuned by the cloud-fit launch's own event time (each
+    // twice) on the updates with measurements after the first kFitTuneAfter, when the maps
+    // have grown (the best split depends on the Gaussians per parent), or fixed by
+    // scphd_set_fit_split.  Every split computes the same values.
+    static constexpr int kFitSplits = 3, kFitTuneAfter = 16;
     const int fit_splits[kFitSplits] = {1, 2, 4};
     bool fit_tuning = true;
+    int fit_seen = 0;   // updates with measurements so far
     int fit_trials = 0, fit_pending = -1, fit_chosen = 0;
     double fit_ms[kFitSplits] = {0, 0, 0};
     cudaEvent_t fit_ev[2] = {nullptr, nullptr};
@@ -401,7 +403,8 @@ public:
             int h = stage_begin(1);
             const double* zs[3] = {M > 0 ? d_stage : nullptr, M > 0 ? d_stage + M : nullptr,
                                    M > 0 ? d_stage + 2 * M : nullptr};
-            const bool fit_timed = fit_tuning && M > 0;
+            const bool fit_timed = fit_tuning && M > 0 && fit_seen >= kFitTuneAfter;
+            if (M > 0) ++fit_seen;
             const int fs = fit_timed ? fit_trials % kFitSplits : fit_chosen, split = fit_splits[fs];
             if (fit_timed) CUDA_TRY(cudaEventRecord(fit_ev[0], stream));
             if (fit_specialised<T>(prm))

@@ -32,6 +32,18 @@ def test_tuned_shapes_leave_results_unchanged(pkg, precision):
             assert np.array_equal(tuned.mixture(1, p), plain.mixture(1, p)), f"frame {k} parent {p}"
     s = tuned.launch_shapes()
     assert s["tuned"] and s["merge_threads"] in (128, 256)
+    # the cloud-fit split is tuned on the updates after the first 16: not yet here
+    assert not s["fit_tuned"] and s["fit_blocks_per_parent"] == 1
+    for k in range(12):   # updates 17-22 tune it (collected at the next update), results unchanged
+        z = sc.frames[k % sc.n_frames]
+        for f in (tuned, plain):
+            f.step(pkg.scene.DT, z[:, 0], z[:, 1], fixed_camera=sc.fixed[k % sc.n_frames], d=z[:, 2])
+        st_a, lw_a = tuned.particles()
+        st_b, lw_b = plain.particles()
+        assert np.array_equal(st_a, st_b) and np.array_equal(lw_a, lw_b), f"extra frame {k}"
+        for p in range(0, cfg.n_parents, 7):
+            assert np.array_equal(tuned.mixture(0, p), plain.mixture(0, p)), f"extra frame {k} parent {p}"
+    s = tuned.launch_shapes()
     assert s["fit_tuned"] and s["fit_blocks_per_parent"] in (1, 2, 4)
 
 
