@@ -200,17 +200,26 @@ __device__ __forceinline__ void ltz_plus_mean(const double* line, const double z
 // 16 bytes (row starts are 16-byte aligned): first the nt pieces of the tail rows (ta,
 // tb), then pieces i0 .. n4-1 of the main rows (a, b) -- the order of one sweep over
 // rows holding all samples, so the sums do not depend on where samples were staged
+// FP32: the partial sums run in pairs through sm_100's packed multiply-add (fma.rn.f32x2:
+// two independent single-precision fused multiply-adds, each rounded as fma.rn.f32), two
+// instructions per piece instead of four, with the same results
+__device__ __forceinline__ unsigned long long pack_f32x2(float lo, float hi) {
+    unsigned long long d;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
+    return d;
+}
 __device__ __forceinline__ float moment_sweep(const float* ta, const float* tb, int nt, const float* a,
                                               const float* b, int i0, int n4) {
-    float s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    unsigned long long s01 = 0ull, s23 = 0ull;   // (s0, s1) and (s2, s3), both +0.0f
     auto piece = [&](const float4 y, const float4 z) {
-        s0 += y.x * z.x;
-        s1 += y.y * z.y;
-        s2 += y.z * z.z;
-        s3 += y.w * z.w;
+        asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(s01) : "l"(pack_f32x2(y.x, y.y)), "l"(pack_f32x2(z.x, z.y)));
+        asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(s23) : "l"(pack_f32x2(y.z, y.w)), "l"(pack_f32x2(z.z, z.w)));
     };
     for (int i = 0; i < nt; ++i) piece(reinterpret_cast<const float4*>(ta)[i], reinterpret_cast<const float4*>(tb)[i]);
     for (int i = i0; i < n4; ++i) piece(reinterpret_cast<const float4*>(a)[i], reinterpret_cast<const float4*>(b)[i]);
+    float s0, s1, s2, s3;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(s0), "=f"(s1) : "l"(s01));
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(s2), "=f"(s3) : "l"(s23));
     return (s0 + s1) + (s2 + s3);
 }
 __device__ __forceinline__ double moment_sweep(const double* ta, const double* tb, int nt, const double* a,
