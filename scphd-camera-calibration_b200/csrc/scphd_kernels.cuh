@@ -306,7 +306,10 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
     __shared__ __align__(16) T s_L[kFitWarps * kFitRound * 28];  // Cholesky factor and mean of merged ones
     __shared__ Pose<T> pose_upd, pose_src;
     __shared__ int s_rd, s_wr;
-    __shared__ T s_fit[kFitWarps * 32];  // per warp: the fitted row (W, pD, mean[6], cov[21])
+    // mean pD of a Gaussian with n of its P samples in view, n = 0..P (P <= 256): the
+    // value n pD / P in FP64, rounded to T, looked up instead of divided per Gaussian
+    __shared__ T s_pbar[257];
+    for (int i = threadIdx.x; i <= P; i += blockDim.x) s_pbar[i] = (T)((double)i * prm.model.pd / (double)P);
     if (threadIdx.x == 0) {
         double zero[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         pose_upd = make_pose<T>(fixed ? zero : b.ext + 12 * p);
@@ -325,7 +328,6 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
     const T invP = T(1) / T(P);
     const T dtT = (T)dt, half_dt2 = T(0.5) * (T)dt * (T)dt;
     const T min_w = (T)prm.min_weight;
-    T* fitw = s_fit + warp * 32;
     T* shw = s_shift + warp * kFitRound * 6;
     T* Lw = s_L + warp * kFitRound * 28;
     // moment owned by this lane: rows (ra, rb) of the product Y[ra] * Y[rb]: lane 0
@@ -503,7 +505,7 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
                 }
                 if (s < P4) stage(Y + s, sY, y, shift, wp);
             }
-            const T pbar = (T)((double)n_in * m.pd / (double)P);
+            const T pbar = s_pbar[n_in];
             const bool raw = !any && n_in > 0 && m.pd > 0.0;
             if (raw) {
                 // the fallback fit (below) needs the raw samples: rare, so they are drawn
@@ -526,6 +528,8 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
             }
             __syncwarp();
             const T* sh = shw + k * 6;
+            // fitted row element `lane` (W, pD, mean[6], packed cov[21]), written from registers
+            T fv = lane == 0 ? W : pbar;
             if (any) {
                 // lane q < 29: moment q over the samples, four partial sums
                 const T mom = lane < 29 ? moment_sweep(Ytk + ra * R, Ytk + rb * R, R / 4, Y + ra * sY, Y + rb * sY,
@@ -544,8 +548,8 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
                     if (ra == a2) da = dvals[a2];
                     if (rb == a2) db = dvals[a2];
                 }
-                if (lane >= 2 && lane < 8) fitw[lane] = sh[lane - 2] + dl;
-                if (lane >= 8 && lane < 29) fitw[lane] = (mom * inv - da * db) * scale;
+                if (lane >= 2 && lane < 8) fv = sh[lane - 2] + dl;
+                if (lane >= 8) fv = (mom * inv - da * db) * scale;
             } else if (pbar > T(0)) {
                 // every sample weighted 1 (exp(LOG0 - LOG0)): unnormalised mean (sum of the
                 // samples) and covariance x (P + P)/P over the valid samples (raw rows)
@@ -567,20 +571,17 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
                     for (int s = 0; s < P; ++s) cva += (Y[ra * sY + s] - ma) * (Y[rb * sY + s] - mb);
                 }
                 const T scale = (T(P) * T(P) + T(P)) / T(P);
-                if (lane < 6) fitw[2 + lane] = mu;
-                if (lane >= 8 && lane < 29) fitw[lane] = cva * scale;
+                const T mu_e = __shfl_sync(0xffffffffu, mu, (lane - 2) & 31);   // mean element lane - 2
+                if (lane >= 2 && lane < 8) fv = mu_e;
+                if (lane >= 8) fv = cva * scale;
                 if (lane == 0) atomicAdd(&b.counters[14], 1ull);
             } else {   // entirely out of view: never used downstream (its log-constant is -inf)
-                if (lane < 6) fitw[2 + lane] = sh[lane];
-                if (lane >= 8 && lane < 29) fitw[lane] = T(0);
+                if (lane >= 2 && lane < 8) fv = sh[lane - 2];
+                if (lane >= 8) fv = T(0);
             }
-            if (lane == 0) fitw[0] = W;
-            if (lane == 1) fitw[1] = pbar;
-            __syncwarp();
-            // fitted row: lane q writes element q (W, pD, mean[6], packed cov[21])
             T* fr = b.fit + ((size_t)p * prm.Gcap + j) * kRow;
-            if (lane < 29) fr[lane] = fitw[lane];
-            __syncwarp();
+            if (lane < 29) fr[lane] = fv;
+            __syncwarp();   // the sweep's reads of the rows end before the next Gaussian's staging
         }
     }
     __syncthreads();
