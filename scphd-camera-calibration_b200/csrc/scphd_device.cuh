@@ -179,6 +179,13 @@ struct Model {   // measurement model constants (FP64 copy; kernels cast to T)
     double fx, fy, u0, v0, B, pd;
     double var[3];   // std_u^2, std_v^2, std_d^2
 };
+// The cloud fit's model constants (the transforms' and the feature noise) rounded to
+// FP32 on the host (the same round-to-nearest as a device cast), read by the FP32
+// kernels straight from the kernel parameters
+struct ModelF {
+    float fx, fy, u0, v0, B, pd;
+    float feat_std[3];
+};
 
 // Weight of a Gaussian's non-detection term, W (1 - mean pD), rounded step by step
 // (no contraction) so that the cloud-fit and merge kernels decide identically
@@ -192,8 +199,8 @@ __device__ __forceinline__ double trcp(double x) { return 1.0 / x; }
 __device__ __forceinline__ float trcp(float x) { return __fdividef(1.0f, x); }
 
 // world point -> (u, v, d, vu, vv, vd), computeMeasurement (:165-196) with baseline B
-template <typename T>
-__device__ inline void measure(const T X[6], const Pose<T>& P, const Model& m, T y[6]) {
+template <typename T, typename M>
+__device__ inline void measure(const T X[6], const Pose<T>& P, const M& m, T y[6]) {
     T d0 = X[0] - P.t[0], d1 = X[1] - P.t[1], d2 = X[2] - P.t[2];
     T x = P.R[0] * d0 + P.R[1] * d1 + P.R[2] * d2;
     T yy = P.R[3] * d0 + P.R[4] * d1 + P.R[5] * d2;
@@ -212,8 +219,8 @@ __device__ inline void measure(const T X[6], const Pose<T>& P, const Model& m, T
 }
 
 // (u, v, d, vu, vv, vd) -> world point, invertMeasurement (:198-217) with baseline B
-template <typename T>
-__device__ inline void invert(const T y[6], const Pose<T>& P, const Model& m, T X[6]) {
+template <typename T, typename M>
+__device__ inline void invert(const T y[6], const Pose<T>& P, const M& m, T X[6]) {
     const T fx = (T)m.fx, fy = (T)m.fy, B = (T)m.B, u0 = (T)m.u0, v0 = (T)m.v0;
     T u = y[0], v = y[1], d = y[2], vu = y[3], vv = y[4], vd = y[5];
     T id = trcp(d), id2 = id * id, r = fx / fy;
@@ -232,8 +239,8 @@ __device__ inline void invert(const T y[6], const Pose<T>& P, const Model& m, T 
     X[5] = P.R[2] * c3 + P.R[5] * c4 + P.R[8] * c5;
 }
 
-template <typename T>
-__device__ inline bool in_range(const T y[6], const Model& m) {   // kernels.cu:37-41
+template <typename T, typename M>
+__device__ inline bool in_range(const T y[6], const M& m) {   // kernels.cu:37-41
     return y[0] >= T(0) && y[0] <= T(2 * m.u0) && y[1] >= T(0) && y[1] <= T(2 * m.v0) && y[2] >= T(0);
 }
 

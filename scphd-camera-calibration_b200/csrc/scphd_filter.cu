@@ -686,6 +686,8 @@ Params make_params(const scphd_config& c) {
     p.var_d0 = c.var_d0; p.var_vu0 = c.var_vu0; p.var_vv0 = c.var_vv0; p.var_vd0 = c.var_vd0;
     for (int i = 0; i < 6; ++i) p.cam_std[i] = c.cam_std[i];
     for (int i = 0; i < 3; ++i) p.feat_std[i] = c.feat_std[i];
+    p.model_f = {(float)p.model.fx, (float)p.model.fy, (float)p.model.u0, (float)p.model.v0, (float)p.model.B,
+                 (float)p.model.pd, {(float)p.feat_std[0], (float)p.feat_std[1], (float)p.feat_std[2]}};
     for (int i = 0; i < 12; ++i) { p.prior_a[i] = c.prior_a[i]; p.prior_b[i] = c.prior_b[i]; }
     p.key0 = (uint32_t)c.seed;
     p.key1 = (uint32_t)(c.seed >> 32);

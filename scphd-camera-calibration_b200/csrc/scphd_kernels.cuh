@@ -26,12 +26,24 @@ namespace scphd {
 struct Params {
     int N, P, Ps, Gcap, Mcap, Scap, K;
     Model model;
+    ModelF model_f;   // model's transform constants in FP32
     double kappa, ps, min_weight, min_sep, min_neff;
     double w0, d0, vu0, vv0, vd0, var_d0, var_vu0, var_vv0, var_vd0;
     double cam_std[6], feat_std[3];
     double prior_a[12], prior_b[12];
     uint32_t key0, key1;
     uint32_t rk[20];   // Philox round keys (key0 + r C0, key1 + r C1), precomputed on the host
+};
+
+// the model constants a kernel in T reads: the FP32 copy, or the FP64 original
+template <typename T> struct ModelOf;
+template <> struct ModelOf<float> {
+    __device__ static const ModelF& get(const Params& prm) { return prm.model_f; }
+    __device__ static float feat_std(const Params& prm, int q) { return prm.model_f.feat_std[q]; }
+};
+template <> struct ModelOf<double> {
+    __device__ static const Model& get(const Params& prm) { return prm.model; }
+    __device__ static double feat_std(const Params& prm, int q) { return prm.feat_std[q]; }
 };
 
 template <typename T> struct Bufs {
@@ -325,6 +337,8 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
     }
     __syncthreads();
     const Model& m = prm.model;
+    // the transforms' constants in T (the FP32 copy needs no conversion per use)
+    const auto& mt = ModelOf<T>::get(prm);
     const T invP = T(1) / T(P);
     const T dtT = (T)dt, half_dt2 = T(0.5) * (T)dt * (T)dt;
     const T min_w = (T)prm.min_weight;
@@ -356,7 +370,7 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
             Pair<T>::two(w1[0], w1[1], z[4], z[5]);
             T yy[6];
             ltz_plus_mean(Lg, z, yy);   // y = L z + mean
-            invert(yy, pose_src, m, X);
+            invert(yy, pose_src, mt, X);
             om = invP;
         } else {         // non-detection cloud carried from the previous frame
             // the previous frame's clouds are only read in this kernel (writes go to
@@ -374,12 +388,12 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
             Pair<T>::two(w[2], w[3], z[2], z[3]);
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
-                T a2 = (T)prm.feat_std[q] * z[q];
+                T a2 = ModelOf<T>::feat_std(prm, q) * z[q];
                 X[q] = X[q] + X[q + 3] * dtT + a2 * half_dt2;
                 X[q + 3] = X[q + 3] + a2 * dtT;
             }
         }
-        measure(X, pose_upd, m, y);
+        measure(X, pose_upd, mt, y);
         return om;
     };
     // the non-detection cloud candidate: predicted world point, weight 1 - pD
@@ -440,8 +454,8 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
 #pragma unroll
                 for (int a2 = 0; a2 < 6; ++a2) { X[a2] = 0; y[a2] = 0; }
             }
-            const bool inr = valid && in_range(y, m);
-            const T pds = inr ? (T)m.pd : T(0);
+            const bool inr = valid && in_range(y, mt);
+            const T pds = inr ? (T)mt.pd : T(0);
             if (valid && wnd) write_nd(j, s, X, pds);
             const T wp = om * pds;
             T shift[6];
@@ -485,8 +499,8 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
 #pragma unroll
                     for (int a2 = 0; a2 < 6; ++a2) { X[a2] = 0; y[a2] = 0; }
                 }
-                const bool inr = valid && in_range(y, m);
-                const T pds = inr ? (T)m.pd : T(0);
+                const bool inr = valid && in_range(y, mt);
+                const T pds = inr ? (T)mt.pd : T(0);
                 n_in += __popc(__ballot_sync(0xffffffffu, inr));
                 if (valid && wnd) write_nd(j, s, X, pds);
                 const T wp = om * pds;
