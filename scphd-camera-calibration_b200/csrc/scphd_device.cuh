@@ -112,14 +112,14 @@ template <> struct Pair<double> {
 };
 template <> struct Pair<float> {
     __device__ static void two(uint32_t wa, uint32_t wb, float& z0, float& z1) {
-        float ua = __fmaf_rn((float)wa, 0x1p-32f, 0x1p-33f);
-        float ub = __fmaf_rn((float)wb, 0x1p-32f, 0x1p-33f);
-        ua = fminf(ua, 0.99999994f);
-        // the approximate log (absolute error up to about 1e-7 near 1) of the largest u_a
+        const float ua = fminf(__fmaf_rn((float)wa, 0x1p-32f, 0x1p-33f), 0.99999994f);
+        // r^2 = -2 ln u_a = (-2 ln 2) log2 u_a, one multiply on the hardware base-2 log.
+        // The approximate log (absolute error up to about 1e-7 near 1) of the largest u_a
         // below 1 can come out as 0 or above: r is 0 there instead of NaN
-        const float r2 = -2.0f * __logf(ua);
+        const float r2 = __log2f(ua) * -1.3862943611198906f;
         const float r = r2 > 0.0f ? r2 * rsqrtf(r2) : 0.0f;
-        float th = 6.283185307179586f * (ub - 0.5f);
+        // the angle 2 pi (u_b - 1/2) = 2 pi ((w_b + 1/2) 2^-32 - 1/2) in one multiply-add
+        const float th = __fmaf_rn((float)wb, 6.283185307179586f * 0x1p-32f, 6.283185307179586f * (0x1p-33f - 0.5f));
         float s, c;
         __sincosf(th, &s, &c);
         z0 = -r * c;
