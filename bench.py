@@ -325,21 +325,38 @@ def run_b200(args):
             eb.synchronize()
             fused_ms += ea.elapsed_time(eb)
             k += 1
-    # end to end through the host-array C ABI: H2D of the frame, step, D2H of the result
+    # end to end through the host-array C ABI: H2D of the frame, step, D2H of the result.
+    # Each step's parent states and log-weights are copied into one of two page-locked
+    # buffers on the filter's stream and read on the host one step later (while the next
+    # step runs); the last step's result is read before the clock stops.
     h2d = d2h = 0
     ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ce0 = filt.counters()
+    N = int(cfg.n_parents)
+    res_bufs = [(torch.empty((N, 12), dtype=torch.float64, pin_memory=True),
+                 torch.empty(N, dtype=torch.float64, pin_memory=True)) for _ in range(2)]
+    res_ev = [torch.cuda.Event(), torch.cuda.Event()]
+    checksum = 0.0
     torch.cuda.synchronize()
     ee0.record(stream)
-    for _ in range(K):
+    for i in range(K):
         z = sc.frames[k]
         filt.step(pkg.scene.DT, z[:, 0], z[:, 1], sc.fixed[k], d=z[:, 2])
-        st, lw = filt.particles()
+        st, lw = res_bufs[i % 2]
+        filt.particles_async(st.data_ptr(), lw.data_ptr())
+        res_ev[i % 2].record(stream)
         h2d += 3 * 8 * z.shape[0]
-        d2h += st.nbytes + lw.nbytes
+        d2h += st.numel() * 8 + lw.numel() * 8
+        if i > 0:   # the previous step's result, on the host
+            res_ev[(i - 1) % 2].synchronize()
+            checksum += float(res_bufs[(i - 1) % 2][1][0])
         k += 1
+    res_ev[(K - 1) % 2].synchronize()
+    checksum += float(res_bufs[(K - 1) % 2][1][0])
     ee1.record(stream)
     ee1.synchronize()
+    if not np.isfinite(checksum):
+        raise RuntimeError("non-finite log-weight read back in the end-to-end pass")
     ce1 = filt.counters()
     e2e_ms = ee0.elapsed_time(ee1)
     e2e_units = int(ce1[6] - ce0[6])

@@ -125,6 +125,14 @@ scphd_status scphd_synchronize(scphd_filter* f);
  * and normalised log-weights (n_parents FP64).  Either pointer may be NULL. */
 scphd_status scphd_get_particles(scphd_filter* f, double* states, double* log_weights);
 
+/* The same copies, queued on the handle's stream (scphd_stream) after the work issued so
+ * far, without waiting for them: the buffers hold the states and log-weights of that
+ * point once scphd_synchronize(f) returns or an event recorded on the stream after this
+ * call has completed.  With page-locked (pinned) buffers the copy overlaps the host's
+ * next calls, so a caller can read step k's result while step k + 1 runs.  The buffers
+ * must stay valid until then.  No reference counterpart (writeMat reads synchronously). */
+scphd_status scphd_get_particles_async(scphd_filter* f, double* states, double* log_weights);
+
 /* Map size of each parent (n_parents int32). */
 scphd_status scphd_get_map_sizes(scphd_filter* f, int32_t* sizes);
 

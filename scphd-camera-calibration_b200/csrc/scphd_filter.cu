@@ -211,6 +211,7 @@ struct scphd_filter {
     virtual scphd_status update_staged(int M, int fixed) = 0;
     virtual scphd_status resample(int32_t* resampled, bool read_back) = 0;
     virtual scphd_status get_particles(double* st, double* lw) = 0;
+    virtual scphd_status get_particles_async(double* st, double* lw) = 0;
     virtual scphd_status get_map_sizes(int32_t* sizes) = 0;
     virtual scphd_status get_map_weights(int p, double* w) = 0;
     virtual scphd_status get_map_clouds(int p, double* xyz, double* om) = 0;
@@ -477,9 +478,14 @@ public:
     }
 
     scphd_status get_particles(double* st, double* lw) override {
+        const scphd_status s = get_particles_async(st, lw);
+        if (s != SCPHD_OK) return s;
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        return SCPHD_OK;
+    }
+    scphd_status get_particles_async(double* st, double* lw) override {
         if (st) CUDA_TRY(cudaMemcpyAsync(st, b.ext, sizeof(double) * 12 * prm.N, cudaMemcpyDeviceToHost, stream));
         if (lw) CUDA_TRY(cudaMemcpyAsync(lw, b.lw, sizeof(double) * prm.N, cudaMemcpyDeviceToHost, stream));
-        CUDA_TRY(cudaStreamSynchronize(stream));
         return SCPHD_OK;
     }
 
@@ -879,6 +885,11 @@ scphd_status scphd_synchronize(scphd_filter* f) {
 scphd_status scphd_get_particles(scphd_filter* f, double* states, double* log_weights) {
     HANDLE(f);
     return f->get_particles(states, log_weights);
+}
+
+scphd_status scphd_get_particles_async(scphd_filter* f, double* states, double* log_weights) {
+    HANDLE(f);
+    return f->get_particles_async(states, log_weights);
 }
 
 scphd_status scphd_get_map_sizes(scphd_filter* f, int32_t* sizes) {

@@ -2224,7 +2224,7 @@ __global__ void __launch_bounds__(256) k_materialize(Params prm, Bufs<T> b, int 
     __shared__ Pose<T> pose_src;
     if (threadIdx.x == 0) pose_src = make_pose<T>(b.map_ext[cur] + 12 * row);
     __syncthreads();
-    const Model& m = prm.model;
+    const auto& m = ModelOf<T>::get(prm);   // the constants the cloud fit regenerates samples with
     const int P = prm.P, Ps = prm.Ps;
     for (int j = warp; j < G; j += blockDim.x >> 5) {
         const size_t erow = (size_t)row * prm.Gcap + j;
@@ -2265,7 +2265,7 @@ __global__ void __launch_bounds__(256) k_materialize(Params prm, Bufs<T> b, int 
                 Pair<T>::two(w[2], w[3], z[2], z[3]);
                 const T dtT = (T)dt, half_dt2 = T(0.5) * (T)dt * (T)dt;
                 for (int q = 0; q < 3; ++q) {
-                    T a = (T)prm.feat_std[q] * z[q];
+                    T a = ModelOf<T>::feat_std(prm, q) * z[q];
                     X[q] = X[q] + X[q + 3] * dtT + a * half_dt2;
                     X[q + 3] = X[q + 3] + a * dtT;
                 }

@@ -208,6 +208,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "scphd_get_fused": (i32, [vp, P(i32)]),
         "scphd_batch_set_fused": (i32, [vp, i32]),
         "scphd_batch_get_fused": (i32, [vp, P(i32)]),
+        "scphd_get_particles_async": (i32, [vp, vp, vp]),
         "scphd_set_fit_split": (i32, [vp, i32]),
         "scphd_get_fit_split": (i32, [vp, P(i32), P(i32)]),
         "scphd_batch_set_fit_split": (i32, [vp, i32]),
@@ -430,6 +431,13 @@ class SCPHDCameraCalibration:
         lw = np.zeros(n, np.float64)
         _check(self._lib.scphd_get_particles(self._h, _dptr(st), _dptr(lw)))
         return st, lw
+
+    def particles_async(self, states_ptr: int, log_weights_ptr: int) -> None:
+        """Queue the copy of the parent states (n x 12 FP64) and log-weights (n FP64) into
+        caller buffers (page-locked for an asynchronous copy) on the filter's stream; they
+        hold the result once work recorded after this call on stream_handle is done."""
+        _check(self._lib.scphd_get_particles_async(self._h, ctypes.c_void_p(states_ptr),
+                                                   ctypes.c_void_p(log_weights_ptr)))
 
     def map_sizes(self) -> np.ndarray:
         s = np.zeros(self.n_parents, np.int32)
