@@ -588,4 +588,27 @@ __device__ __forceinline__ T log_term(T c, const T* Si, const T* mu, const T* z)
     return c - T(0.5) * q;
 }
 
+// FP32 likelihood terms in base 2: with c2 = log2(e) c and A = S^-1 scaled by -log2(e)/2
+// on the diagonal and -log2(e) off it (packed as S^-1), log2 of a pair's term is
+// c2 + sum_a n_a (sum_{b >= a} A_ab n_b), n = z - mean: nine multiply-adds for K = 3
+template <int K>
+__device__ __forceinline__ float log2_term(float c2, const float* A, const float* mu, const float* z) {
+    const float n0 = z[0] - mu[0], n1 = z[1] - mu[1];
+    if (K == 2) {
+        const float u0 = fmaf(A[1], n1, A[0] * n0);
+        return fmaf(n1, A[2] * n1, fmaf(n0, u0, c2));
+    }
+    const float n2 = z[2] - mu[2];
+    const float u0 = fmaf(A[3], n2, fmaf(A[1], n1, A[0] * n0));
+    const float u1 = fmaf(A[4], n2, A[2] * n1);
+    return fmaf(n2, A[5] * n2, fmaf(n1, u1, fmaf(n0, u0, c2)));
+}
+constexpr float kLog2e = 1.4426950408889634f, kLn2 = 0.6931471805599453f;
+// 2^x by the hardware approximation (max 2 ulp; 0 below the normal range)
+__device__ __forceinline__ float exp2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 }  // namespace scphd

@@ -640,7 +640,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
 // rows of its Gaussians -- contiguous in global memory -- out with coalesced stores:
 //   prep row (kPrep): the gain and posterior covariance the merge reads per survivor;
 //   likelihood row (kLikTerms): log-constant (-inf when the posterior is not PD), PD
-//   flag, packed S^-1, mean (u, v, d) -- the k_likelihood terms, read in 16-byte pieces.
+//   flag, packed S^-1, mean (u, v, d) -- the k_likelihood terms, read in 16-byte pieces;
+//   in FP32 in base 2 (log2(e) c, S^-1 scaled for log2_term).
 constexpr int kLikTerms = 12;   // log-constant, PD flag, S^-1 (6), mean (3), pad: 16-byte pieces
 constexpr int kPrepThreads = 128;
 constexpr int kPrepStride = kPrep + 1, kLikStride = kLikTerms + 1;
@@ -688,6 +689,14 @@ __device__ __forceinline__ void prep_body(const Params& prm, const Bufs<T>& b, i
             l[1] = d[1];
 #pragma unroll
             for (int i = 0; i < 6; ++i) l[2 + i] = d[kPrepSi + i];
+            if constexpr (sizeof(T) == 4) {   // base-2 form (log2_term): c2 and the scaled S^-1
+                l[0] = l[0] * kLog2e;
+#pragma unroll
+                for (int i = 0; i < 6; ++i) {
+                    const bool diag = K == 3 ? (i == 0 || i == 2 || i == 5) : (i == 0 || i == 2);
+                    l[2 + i] = l[2 + i] * (diag ? -0.5f * kLog2e : -kLog2e);
+                }
+            }
 #pragma unroll
             for (int a = 0; a < 3; ++a) l[8 + a] = v[2 + a];
             l[11] = T(0);
@@ -783,8 +792,21 @@ __device__ __forceinline__ void likelihood_body(const Params& prm, const Bufs<T>
 #pragma unroll
         for (int a2 = 0; a2 < K; ++a2) zm[a2] = b.z[m * 3 + a2];
     }
-    const T bpc = (T)log((double)M * prm.w0 + prm.kappa);
-    const T cand_min = bpc + (T)log(prm.min_weight) - T(1);
+    // the pair terms' base: log2 in FP32 (log2_term on the rows k_prep scaled), ln in FP64;
+    // sc = the factor from ln to that base, ic its inverse
+    constexpr bool kB2 = sizeof(T) == 4;
+    const T sc = kB2 ? T(kLog2e) : T(1), ic = kB2 ? T(kLn2) : T(1);
+    auto pair_term = [&](const T* t) -> T {
+        if constexpr (kB2) return log2_term<K>(t[0], t + 2, t + 8, zm);
+        else return log_term<T, K>(t[0], t + 2, t + 8, zm);
+    };
+    auto exp_w = [&](T x) -> T {   // base^x for the normaliser sums and survivor weights
+        if constexpr (kB2) return exp2_approx(x);
+        else return texp_sum(x);
+    };
+    const T bpc = (T)log((double)M * prm.w0 + prm.kappa);   // ln of the birth + clutter term
+    const T bpc_w = bpc * sc;
+    const T cand_min = (bpc + (T)log(prm.min_weight) - T(1)) * sc;
     int* s_cand = reinterpret_cast<int*>(s_terms + (size_t)prm.Gcap * kLikTerms);   // [slot][thread]
     int n_cand = 0;
     // largest log-constant of the parent: lt_j <= c_j, since the quadratic form is >= 0
@@ -802,17 +824,17 @@ __device__ __forceinline__ void likelihood_body(const Params& prm, const Bufs<T>
     // otherwise (a log-constant far above bpc), and always in FP64, by an online
     // log-sum-exp around the running maximum, whose dominant term is exp(0) = 1 exactly:
     // a weight near 1 then rounds as in the FP64 oracle, and the merge order of nearly
-    // tied weights with it.
-    const T s0 = cm > bpc ? cm : bpc;
-    const bool fixed_shift = sizeof(T) == 4 && !(cm - bpc > T(60));
+    // tied weights with it.  (FP32 values are in base 2 here, the limits scaled alike.)
+    const T s0 = cm > bpc_w ? cm : bpc_w;
+    const bool fixed_shift = kB2 && !(cm - bpc_w > T(60) * sc);
     T mx = tneg_inf<T>(), acc = 0;
     if (m < M) {
         if (fixed_shift) {
             for (int k = 0; k < G; ++k) {
                 T t[kLikTerms];
                 load_terms(s_terms + (size_t)k * kLikTerms, t);
-                const T lt = log_term<T, K>(t[0], t + 2, t + 8, zm);   // -inf for a non-PD posterior
-                acc += texp_sum(lt - s0);
+                const T lt = pair_term(t);   // -inf for a non-PD posterior
+                acc += exp_w(lt - s0);
                 if (lt >= cand_min) {
                     if (n_cand < kLikCand) s_cand[n_cand * blockDim.x + threadIdx.x] = k;
                     ++n_cand;
@@ -824,9 +846,9 @@ __device__ __forceinline__ void likelihood_body(const Params& prm, const Bufs<T>
                 load_terms(s_terms + (size_t)k * kLikTerms, t);
                 const T c = t[0];
                 if (!(c > tneg_inf<T>())) continue;
-                const T lt = log_term<T, K>(c, t + 2, t + 8, zm);
-                if (lt > mx) { acc = acc * texp_sum(mx - lt) + T(1); mx = lt; }   // online log-sum-exp
-                else acc += texp_sum(lt - mx);
+                const T lt = pair_term(t);
+                if (lt > mx) { acc = acc * exp_w(mx - lt) + T(1); mx = lt; }   // online log-sum-exp
+                else acc += exp_w(lt - mx);
                 if (lt >= cand_min) {
                     if (n_cand < kLikCand) s_cand[n_cand * blockDim.x + threadIdx.x] = k;
                     ++n_cand;
@@ -834,14 +856,24 @@ __device__ __forceinline__ void likelihood_body(const Params& prm, const Bufs<T>
             }
         }
     }
-    T ell = bpc;
+    // the normaliser in the working base (ell_w), stored as ln: (sum_j base^lt_j) (+) bpc
+    auto log_b = [&](T x) -> T {   // accurate log in the working base
+        if constexpr (kB2) return log2f(x);
+        else return tlog(x);
+    };
+    auto exp_b = [&](T x) -> T {   // accurate base^x
+        if constexpr (kB2) return exp2f(x);
+        else return texp(x);
+    };
+    T ell_w = bpc_w;
     if (m < M && fixed_shift) {
-        ell = s0 + tlog(acc + texp(bpc - s0));   // (sum_j exp(lt_j)) (+) bpc
+        ell_w = s0 + log_b(acc + exp_b(bpc_w - s0));
     } else if (m < M && mx > tneg_inf<T>()) {
-        // (sum_j exp(lt_j)) (+) bpc, evaluated around the larger of the two
-        T big = mx > bpc ? mx : bpc;
-        ell = big + tlog(acc * texp(mx - big) + texp(bpc - big));
+        // evaluated around the larger of the two
+        T big = mx > bpc_w ? mx : bpc_w;
+        ell_w = big + log_b(acc * exp_b(mx - big) + exp_b(bpc_w - big));
     }
+    const T ell = kB2 ? ell_w * ic : ell_w;
     if (m < M) b.ell[(size_t)p * prm.Mcap + m] = ell;
     // survivors among the candidates (or all pairs, if the list overflowed)
     const T minw = (T)prm.min_weight;
@@ -855,7 +887,7 @@ __device__ __forceinline__ void likelihood_body(const Params& prm, const Bufs<T>
             load_terms(s_terms + (size_t)k * kLikTerms, t);
             const T c = t[0];
             if (!(c > tneg_inf<T>() && t[1] > T(0))) continue;
-            const T w = texp_sum(log_term<T, K>(c, t + 2, t + 8, zm) - ell);
+            const T w = exp_w(pair_term(t) - ell_w);
             if (w >= minw) {
                 const int slot = atomicAdd(&b.surv_n[p], 1);
                 if (slot < prm.Scap) {
