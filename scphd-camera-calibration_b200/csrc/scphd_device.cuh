@@ -133,9 +133,9 @@ template <> __device__ __forceinline__ double tsqrt(double x) { return sqrt(x); 
 template <typename T> __device__ __forceinline__ T texp(T x);
 template <> __device__ __forceinline__ float texp(float x) { return expf(x); }
 template <> __device__ __forceinline__ double texp(double x) { return exp(x); }
-// exp for the likelihood's normaliser sums and survivor weights: in FP32 the hardware
-// base-2 exponential of x log2(e) (__expf: relative error about 2 ulp + |x| 2^-22,
-// inside the FP32 mode's tolerance), in FP64 the correctly rounded exp
+// exp for the FP64 likelihood's normaliser sums and survivor weights (the FP32
+// likelihood works in base 2, exp2_approx); the FP32 form is the hardware base-2
+// exponential of x log2(e) (__expf: relative error about 2 ulp + |x| 2^-22)
 __device__ __forceinline__ float texp_sum(float x) { return __expf(x); }
 __device__ __forceinline__ double texp_sum(double x) { return exp(x); }
 template <typename T> __device__ __forceinline__ T tlog(T x);
