@@ -465,7 +465,12 @@ public:
     scphd_status resample(int32_t* resampled, bool read_back) override {
         int h = stage_begin(5);
         k_resample<<<1, 1024, 0, stream>>>(prm, b.lw, b.ext, b.ext_tmp, b.src, b.src_tmp, b.cum, b.scal, b.flags,
-                                           b.resample_idx, frame, 0, -1.0, b.counters);
+                                           b.resample_idx, frame, 0, -1.0, b.counters, 0);
+        LAUNCHED();
+        const int ng = (12 * prm.N + 255) / 256;
+        k_gather_parents<<<ng, 256, 0, stream>>>(b.flags, b.resample_idx, b.ext, b.ext_tmp, prm.N);
+        LAUNCHED();
+        k_copy_parents<<<ng, 256, 0, stream>>>(b.flags, b.ext_tmp, b.ext, prm.N);
         LAUNCHED();
         stage_end(h);
         if (read_back) {
@@ -1212,7 +1217,7 @@ scphd_status scphd_systematic_resample(const double* weights, int32_t n, double 
         cudaMemset(d_ext, 0, 96 * (size_t)n);
         cudaMemset(d_src, 0, 4 * n);
         k_resample<<<1, 1024>>>(prm, d_lw, d_ext, d_ext_tmp, d_src, d_src_tmp, d_cum, d_scal, d_flags, d_idx, 0, 1,
-                                u01v, nullptr);
+                                u01v, nullptr, 1);
         g_launches.fetch_add(1, std::memory_order_relaxed);
         cudaError_t e = cudaDeviceSynchronize();
         if (e != cudaSuccess) {

@@ -2106,10 +2106,12 @@ __device__ void block_scan_inclusive(double* data, int N, double* s_tmp) {
     __syncthreads();
 }
 
+// gather_ext = false: the parent states are left for k_gather_parents / k_copy_parents
+// (the single filter's path: the 96-byte rows are moved by the whole GPU, not one block)
 __device__ __forceinline__ void resample_body(const Params& prm, double* lw, double* ext, double* ext_tmp, int* src,
                                               int* src_tmp, double* cum, double* scal, int* flags, int* idx_out,
                                               uint32_t frame, int force, double r0_override,
-                                              unsigned long long* counters) {
+                                              unsigned long long* counters, bool gather_ext = true) {
     __shared__ double s_tmp[32];
     __shared__ double s_r0;
     __shared__ int s_amax;
@@ -2182,13 +2184,15 @@ __device__ __forceinline__ void resample_body(const Params& prm, double* lw, dou
         int i = lo < N ? lo : s_amax;
         i = i < 0 ? 0 : (i >= N ? N - 1 : i);
         idx_out[j] = i;
-        for (int q = 0; q < 12; ++q) ext_tmp[12 * j + q] = ext[12 * i + q];
+        if (gather_ext)
+            for (int q = 0; q < 12; ++q) ext_tmp[12 * j + q] = ext[12 * i + q];
         src_tmp[j] = src[i];
     }
     __syncthreads();
     const double lw0 = -log((double)N);
     for (int j = threadIdx.x; j < N; j += blockDim.x) {
-        for (int q = 0; q < 12; ++q) ext[12 * j + q] = ext_tmp[12 * j + q];
+        if (gather_ext)
+            for (int q = 0; q < 12; ++q) ext[12 * j + q] = ext_tmp[12 * j + q];
         src[j] = src_tmp[j];
         lw[j] = lw0;
     }
@@ -2201,8 +2205,24 @@ __device__ __forceinline__ void resample_body(const Params& prm, double* lw, dou
 __global__ void __launch_bounds__(1024) k_resample(__grid_constant__ const Params prm, double* lw, double* ext,
                                                    double* ext_tmp, int* src, int* src_tmp, double* cum, double* scal,
                                                    int* flags, int* idx_out, uint32_t frame, int force,
-                                                   double r0_override, unsigned long long* counters) {
-    resample_body(prm, lw, ext, ext_tmp, src, src_tmp, cum, scal, flags, idx_out, frame, force, r0_override, counters);
+                                                   double r0_override, unsigned long long* counters, int gather_ext) {
+    resample_body(prm, lw, ext, ext_tmp, src, src_tmp, cum, scal, flags, idx_out, frame, force, r0_override, counters,
+                  gather_ext != 0);
+}
+
+// The resampled parents' states, for a k_resample launch with gather_ext = 0: one thread
+// per state value, ext_tmp[j] = ext[idx[j]], then ext = ext_tmp (when flags[0] says the
+// step resampled; otherwise both return at once)
+__global__ void k_gather_parents(const int* flags, const int* idx, const double* ext, double* ext_tmp, int N) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (!flags[0] || e >= 12 * N) return;
+    const int j = e / 12;
+    ext_tmp[e] = ext[12 * idx[j] + (e - 12 * j)];
+}
+__global__ void k_copy_parents(const int* flags, const double* ext_tmp, double* ext, int N) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (!flags[0] || e >= 12 * N) return;
+    ext[e] = ext_tmp[e];
 }
 
 template <typename T>
