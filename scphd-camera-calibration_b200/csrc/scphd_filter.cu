@@ -1289,7 +1289,9 @@ template <typename T> struct Batch final : scphd_batch {
     bool use_graph = false;
     bool captured = false;
     cudaGraphExec_t exec = nullptr;
-    cudaEvent_t done = nullptr;
+    // recorded after a step's copies out of the pinned buffers: the next step rewrites
+    // them once these copies are done, while the previous step's kernels may still run
+    cudaEvent_t copied = nullptr;
     std::vector<Group> groups;
     FrameArgs* h_fa = nullptr;    // pinned, one per filter
     FrameArgs* d_fa = nullptr;
@@ -1335,7 +1337,7 @@ template <typename T> struct Batch final : scphd_batch {
         for (cudaEvent_t e : fit_ev)
             if (e) cudaEventDestroy(e);
         if (exec) cudaGraphExecDestroy(exec);
-        if (done) cudaEventDestroy(done);
+        if (copied) cudaEventDestroy(copied);
         if (h_fa) cudaFreeHost(h_fa);
         if (h_stage) cudaFreeHost(h_stage);
         if (dev_mem) cudaFree(dev_mem);
@@ -1355,7 +1357,7 @@ template <typename T> struct Batch final : scphd_batch {
         const int F = (int)fs.size();
         K = fs[0]->prm.K;
         CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-        CUDA_TRY(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&copied, cudaEventDisableTiming));
         CUDA_TRY(cudaEventCreate(&tune_ev[0]));
         CUDA_TRY(cudaEventCreate(&tune_ev[1]));
         CUDA_TRY(cudaEventCreate(&fit_ev[0]));
@@ -1576,11 +1578,15 @@ template <typename T> struct Batch final : scphd_batch {
         return SCPHD_OK;
     }
 
-    scphd_status enqueue() {
+    // the step's measurements and frame arguments to the device, ahead of its kernels on
+    // the stream (outside the graph, which holds the kernels only)
+    scphd_status copy_in() {
         CUDA_TRY(cudaMemcpyAsync(d_stage, h_stage, sizeof(double) * stage_total, cudaMemcpyHostToDevice, stream));
         CUDA_TRY(cudaMemcpyAsync(d_fa, h_fa, sizeof(FrameArgs) * fs.size(), cudaMemcpyHostToDevice, stream));
-        return K == 2 ? launch_all<2>() : launch_all<3>();
+        CUDA_TRY(cudaEventRecord(copied, stream));
+        return SCPHD_OK;
     }
+    scphd_status enqueue() { return K == 2 ? launch_all<2>() : launch_all<3>(); }
 
     scphd_status step(double dt, const scphd_frame* frames, bool device_frames) override {
         const int F = (int)fs.size();
@@ -1596,8 +1602,9 @@ template <typename T> struct Batch final : scphd_batch {
                     if (!std::isfinite(fr.u[i]) || !std::isfinite(fr.v[i]) || (K == 3 && !std::isfinite(fr.d[i])))
                         return fail(SCPHD_ERR_INVALID, "non-finite measurement");
         }
-        // the pinned buffers are rewritten: the previous step must have consumed them
-        CUDA_TRY(cudaEventSynchronize(done));
+        // the pinned buffers are rewritten: the previous step's copies out of them must be
+        // done (its kernels may still run: this step's host work overlaps them)
+        CUDA_TRY(cudaEventSynchronize(copied));
         for (int f = 0; f < F; ++f) {
             Filter<T>* fl = filt(f);
             if (fl->pending) {   // a predict() issued outside the batch: apply it first
@@ -1637,6 +1644,10 @@ template <typename T> struct Batch final : scphd_batch {
             const scphd_status ts = tune_collect();
             if (ts != SCPHD_OK) return ts;
         }
+        {
+            const scphd_status cs = copy_in();
+            if (cs != SCPHD_OK) return cs;
+        }
         if (use_graph && !tuning && !fit_tuning) {
             if (!captured) {
                 cudaGraph_t g = nullptr;
@@ -1660,7 +1671,6 @@ template <typename T> struct Batch final : scphd_batch {
             scphd_status s = enqueue();
             if (s != SCPHD_OK) return s;
         }
-        CUDA_TRY(cudaEventRecord(done, stream));
         for (int f = 0; f < F; ++f) {
             Filter<T>* fl = filt(f);
             fl->cur ^= 1;

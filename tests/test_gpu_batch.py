@@ -119,6 +119,28 @@ def test_batch_matches_filters_alone(pkg, use_graph, precision, fused):
         _assert_same(_state(alone[i]), _state(batched[i]), f"after batch member {i}")
 
 
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_batch_steps_back_to_back(pkg, use_graph):
+    """Host-frame batch steps queued without waiting in between: a step refills the
+    page-locked frame buffers once the previous step's copies are done, while its kernels
+    may still run, so every member must still end where it gets alone."""
+    _need_gpu()
+    members = _members(pkg, 1)
+    alone = [pkg.SCPHDCameraCalibration(cfg) for _, cfg in members]
+    batched = [pkg.SCPHDCameraCalibration(cfg) for _, cfg in members]
+    batch = pkg.SCPHDBatch(batched, use_graph=use_graph)
+    for k in range(6):
+        frames = [_frame(sc, k, i, 3) for i, (sc, _) in enumerate(members)]
+        for f, (u, v, d, fixed) in zip(alone, frames):
+            f.step(0.5, u, v, fixed_camera=fixed, d=d)
+        batch.step(0.5, [(np.ascontiguousarray(u), np.ascontiguousarray(v), np.ascontiguousarray(d), fixed)
+                         for u, v, d, fixed in frames])
+    batch.synchronize()
+    for i in range(3):
+        _assert_same(_state(alone[i]), _state(batched[i]), f"member {i}")
+    batch.close()
+
+
 def test_batch_two_dim_and_device_frames(pkg):
     _need_gpu()
     import torch
