@@ -429,9 +429,20 @@ def run_b200(args):
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp) and args.workload == "plain_c1" and not args.parents:
         with open(tp) as fh:
-            tr = json.load(fh).get(name)
+            tj = json.load(fh)
+        tr = tj.get(name)
         if tr:
             traffic = tr.get("bytes_per_launch_scaled")
+        # issue side of the cloud fit: the warp instructions per fitted Gaussian of the
+        # recorded capture x the Gaussians fitted per launch, over the launch's issue slots
+        # (148 SMs x 4 schedulers x the median SM clock sampled in the timed region)
+        ti = tj.get("cloud_fit_issue")
+        if ti and name == "cloud_fit" and avg_ms > 0 and clk and clk.get("sm_mhz"):
+            inst = ti["warp_instructions_per_gaussian"] * fitted / max(1, K)
+            slots = 148 * 4 * clk["sm_mhz"] * 1e6 * avg_ms / 1e3
+            compute["issue"] = {"warp_instructions_per_launch": inst, "issue_slots_per_launch": slots,
+                                "frac": inst / slots,
+                                "instructions_source": "profiles/k_cloud_fit_plain_c1_512parents.md"}
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:

@@ -305,7 +305,10 @@ typedef struct scphd_batch scphd_batch;
 scphd_status scphd_batch_create(scphd_filter* const* filters, int32_t n_filters, int32_t use_graph,
                                 scphd_batch** out);
 scphd_status scphd_batch_destroy(scphd_batch* b);
-/* frames[i] is filter i's frame; arrays in HOST memory (copied during the call). */
+/* frames[i] is filter i's frame; arrays in HOST memory (copied during the call).  The
+ * step is queued on the batch's stream and the call returns; the next call waits only
+ * until this step's frame copies have run (not its kernels), so consecutive steps
+ * overlap their host work with the previous step's kernels. */
 scphd_status scphd_batch_step(scphd_batch* b, double dt, const scphd_frame* frames);
 /* As scphd_batch_step with the frames' arrays in DEVICE memory (read by the kernels;
  * keep them unchanged until the step has run on the batch's stream). */
