@@ -322,10 +322,11 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
     // value n pD / P in FP64, rounded to T, looked up instead of divided per Gaussian
     __shared__ T s_pbar[257];
     for (int i = threadIdx.x; i <= P; i += blockDim.x) s_pbar[i] = (T)((double)i * prm.model.pd / (double)P);
+    // the two poses (FP64 rotation terms) by threads of two warps, side by side
+    if (threadIdx.x == 32) pose_src = make_pose<T>(b.map_ext[cur] + 12 * row);
     if (threadIdx.x == 0) {
         double zero[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
         pose_upd = make_pose<T>(fixed ? zero : b.ext + 12 * p);
-        pose_src = make_pose<T>(b.map_ext[cur] + 12 * row);
         if (c == 0) {
             b.surv_n[p] = 0;
             atomicAdd(&b.counters[4], (unsigned long long)G * (unsigned long long)M);
@@ -428,14 +429,22 @@ __device__ __forceinline__ void cloud_fit_body(const Params& prm, const Bufs<T>&
             atomicAdd(&s_rd, nR - __popc(merged));
             atomicAdd(&s_wr, __popc(writes));
         }
-        for (unsigned mk = merged; mk; mk &= mk - 1) {   // Cholesky factor (21, stored in the map row) and mean (6)
-            const int k = __ffs(mk) - 1;
-            const T* ent = b.map[cur] + ((size_t)row * prm.Gcap + gw + nwp * (k0 + k)) * kRow;
-            T* Lk = Lw + k * 28;
-            if (lane < 21) Lk[lane] = ent[7 + lane];
-            else if (lane < 27) Lk[lane] = ent[1 + lane - 21];
-            else if (lane == 27) Lk[27] = T(0);
+        // Cholesky factor (21, stored in the map row) and mean (6) of the round's merged
+        // Gaussians: every load issued before the first store (the previous frame's map
+        // is only read in this kernel), lane e holding element e of each
+        T lv[kFitRound];
+#pragma unroll
+        for (int k = 0; k < kFitRound; ++k) {
+            lv[k] = T(0);
+            if ((merged >> k) & 1u) {
+                const T* ent = b.map[cur] + ((size_t)row * prm.Gcap + gw + nwp * (k0 + k)) * kRow;
+                if (lane < 21) lv[k] = __ldg(ent + 7 + lane);
+                else if (lane < 27) lv[k] = __ldg(ent + 1 + lane - 21);
+            }
         }
+#pragma unroll
+        for (int k = 0; k < kFitRound; ++k)
+            if (((merged >> k) & 1u) && lane < 28) Lw[k * 28 + lane] = lv[k];
         __syncwarp();
         // tail pass: samples [0, R) of the round's Gaussians; lane gi * R (sample 0)
         // gives its Gaussian's shift
