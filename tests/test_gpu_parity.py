@@ -366,8 +366,8 @@ def test_fp64_capped_maps_match_oracle(pkg, orc):
     assert c[1] == 0, "survivor scratch overflow"
 
 
-def test_fp64_config0_all_frames_match_oracle(pkg, orc):
-    """BASELINE config 0 in full: 256 parents, 50 landmarks, clutter 10/frame,
+def test_fp64_plain_c0_all_frames_match_oracle(pkg, orc):
+    """The plain_c0 workload in full: 256 parents, 50 landmarks, clutter 10/frame,
     <= 64 Gaussians per parent, 100 samples per Gaussian, all 100 frames, FP64,
     compared with the oracle after every frame.  The cap binds on every parent from
     about frame 10 on."""
